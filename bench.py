@@ -1,0 +1,370 @@
+#!/usr/bin/env python
+"""Points x iterations per second of the bundling loop on the large workload.
+
+Workload: 100,000 seeded random-walk polylines (2..8 control points each),
+4.95M samples at spacing 1/1000 of the canvas, 2048^2 density grid, blur
+sigma 16 px, neighbour radius 16 texels (synthetic stand-in for the
+reference's datasets, which are LFS stubs). A step is one bundling iteration
+(Gpu::iterate: neighbour mean fused with the splat, grid rebuild, blur,
+normalisation) with all data resident in HBM; the step's working set
+(~330 MB) is larger than the 126 MB L2.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Under torchrun every rank runs an independent replica (the path does not
+shard; scaling is weak) and rank 0 prints one JSON line. `--impl reference`
+times the CPU restatement of the reference's algorithm (the reference itself
+is Rust + wgpu and cannot run here) on the host cores, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "points·iter/s at 100k edges"
+UNIT = "points·iter/s"
+ITERATIONS_PER_JOB = 30
+# Algorithmic bytes per sample of the fused neighbour-mean kernel: read
+# position 8 + fixed-point position 8 + tag 4; write position 8 + tag 4 +
+# next search cell 4; population atomic 4 + splat atomic 4.
+MEAN_BYTES_PER_SAMPLE = 44
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=200)
+    p.add_argument("--warmup", type=int, default=10)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--edges", type=int, default=100_000)
+    p.add_argument("--e2e-jobs", type=int, default=3)
+    p.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU work of the baseline sample")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+# ---------------------------------------------------------------- ranks
+class Ranks:
+    def __init__(self, want: int):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.dist = None
+        if self.world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+
+            backend = "nccl" if torch.cuda.is_available() else "gloo"
+            if backend == "nccl":
+                torch.cuda.set_device(self.local)
+            dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=300))
+            self.dist = dist
+            self.torch = torch
+            self.backend = backend
+
+    def _t(self, x):
+        t = self.torch.tensor([float(x)], dtype=self.torch.float64)
+        return t.cuda() if self.backend == "nccl" else t
+
+    def barrier(self):
+        if self.dist:
+            self.dist.barrier()
+
+    def max(self, x: float) -> float:
+        if not self.dist:
+            return x
+        t = self._t(x)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, x: float) -> float:
+        if not self.dist:
+            return x
+        t = self._t(x)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self):
+        if self.dist:
+            self.dist.barrier()
+            self.dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=5)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() in ("active", "1"):
+                    reasons.add(name)
+        return {
+            "sm_mhz": statistics.median(sm) if sm else None,
+            "sm_max_mhz": max(smax) if smax else None,
+            "reasons": sorted(reasons),
+            "samples": len(sm),
+        }
+
+
+def measured_peak_hbm():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """DRAM bytes per launch of the neighbour-mean kernel from the committed
+    ncu summary (profiles/neighbor_mean_large.json), or None."""
+    path = os.path.join(ROOT, "profiles", "neighbor_mean_large.json")
+    try:
+        with open(path) as f:
+            return json.load(f).get("dram_bytes_per_launch")
+    except (OSError, ValueError):
+        return None
+
+
+def scan_launches(n: int) -> int:
+    tile = 2048
+    if n <= tile:
+        return 1
+    return 2 + scan_launches((n + tile - 1) // tile)
+
+
+def workload(edges: int):
+    from bundling_thingy_b200 import synthetic
+
+    return synthetic.large(edges)
+
+
+# ---------------------------------------------------------------- CPU sample
+def cpu_sample(w, target_seconds: float, steps: int = 1, warmup: int = 0, threads: int = 0):
+    """Bounded CPU timing of the oracle (the reference's algorithm restated):
+    neighbour mean of every s-th sample (s chosen so one step is about
+    target_seconds) plus a full density pass charged pro rata."""
+    import oracle as O
+
+    threads = threads or len(os.sched_getaffinity(0))
+    cfg = O.Config(w.width, w.height, radius=w.radius, resample_scale=(500.0, 500.0),
+                   sigma=float(np.float32(w.sigma)), threads=threads)
+    pipe = O.Pipeline(cfg)
+    n = pipe.upload(w.xy, w.starts)
+    xy, _ = pipe.points()
+    mv = O.movable_mask(pipe.paths(), n)
+    taps = O.blur_weights(float(np.float32(w.sigma)))
+    # Calibrate the stride on a small probe (query time only).
+    probe = max(1, n // 2000)
+    _, done, t_index, t_call = O.neighbor_mean_sample(xy, mv, w.width, w.height, w.radius, probe, threads)
+    per_sample = max(t_call - t_index, 1e-9) / max(done, 1)
+    stride = max(1, int(np.ceil(n * per_sample / target_seconds)))
+    sampled = (n + stride - 1) // stride
+    values = []
+    for i in range(warmup + steps):
+        out, done, t_index, t_call = O.neighbor_mean_sample(xy, mv, w.width, w.height, w.radius, stride, threads)
+        t_query = max(t_call - t_index, 0.0)
+        t0 = time.perf_counter()
+        counts = O.splat(out, w.width, w.height)
+        _, vt, peak = O.blur(counts, w.width, w.height, taps)
+        O.normalize(vt, peak)
+        t_density = time.perf_counter() - t0
+        # The sampled samples over their query time plus the whole-set grid
+        # index and density pass charged for their share of the samples.
+        share = sampled / n
+        if i >= warmup:
+            values.append(sampled / (t_query + (t_index + t_density) * share))
+    return {
+        "value": float(statistics.median(values)),
+        "unit": UNIT,
+        "cores": threads,
+        "kind": "port",
+        "sample": (f"neighbour mean of the first {sampled} of {n} samples (whole paths) of the large workload "
+                   f"+ the whole-set grid index and density pass charged pro rata, "
+                   f"{steps} step(s), OpenMP over {threads} host threads"),
+    }
+
+
+# ---------------------------------------------------------------- reference arm
+def run_reference(args, ranks: Ranks):
+    if ranks.rank != 0:
+        return
+    w = workload(args.edges)
+    base = cpu_sample(w, target_seconds=2.0, steps=args.steps, warmup=args.warmup)
+    line = {
+        "impl": "reference",
+        "metric": METRIC, "value": base["value"], "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded random-walk polylines; reference datasets are LFS stubs)",
+        "config": {"workload": "large: 100k polylines, 4.95M samples, 2048^2, sigma 16, radius 16",
+                   "iterations_per_job": ITERATIONS_PER_JOB},
+        "cpu_baseline": base,
+        "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": ("the reference is Rust + wgpu/Vulkan (no rustc, no graphics stack on this box); "
+                 "its algorithm is timed through the CPU restatement in oracle/"),
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- our arm
+def run_ours(args, ranks: Ranks):
+    import bundling_thingy_b200 as bt
+
+    w = workload(args.edges)
+    device = ranks.local
+    opts = bt.Options(width=w.width, height=w.height, neighbor_radius=w.radius, sample_spacing=w.spacing,
+                      blur_sigma=w.sigma, device=device, timing=True)
+    gpu = bt.Gpu(opts)
+    n = gpu.upload((w.xy, w.starts))
+    info = gpu.info()
+    sampler = ClockSampler(device)
+    sampler.start()
+    gpu.iterate(args.warmup)
+    ranks.barrier()
+    gpu.synchronize()
+    ms = gpu.iterate_timed(args.steps)
+    gpu.synchronize()
+    ranks.barrier()
+    clocks = sampler.stop()
+    stages = gpu.stage_times()
+    ms_max = ranks.max(ms)
+    points = ranks.sum(float(n) * args.steps)
+    value = points / (ms_max / 1e3)
+
+    mean_ms = stages.get("graph.neighbor_mean", float("nan")) / args.steps
+    peak, peak_kind = measured_peak_hbm()
+    bytes_per_launch = MEAN_BYTES_PER_SAMPLE * n
+    achieved = bytes_per_launch / (mean_ms / 1e3) / 1e9
+    total_stage = sum(stages.values())
+    gpu.close()
+
+    # End to end through the public API with host buffers: upload the control
+    # points, 30 iterations, read back the 12-byte records and the density.
+    opts_e2e = bt.Options(width=w.width, height=w.height, neighbor_radius=w.radius, sample_spacing=w.spacing,
+                          blur_sigma=w.sigma, device=device)
+    e2e_gpu = bt.Gpu(opts_e2e)
+    records = np.empty(12 * n, np.uint8)
+    job_times = []
+    for j in range(args.e2e_jobs + 1):
+        ranks.barrier()
+        t0 = time.perf_counter()
+        m = e2e_gpu.upload((w.xy, w.starts))
+        e2e_gpu.iterate(ITERATIONS_PER_JOB)
+        bt.library().bt_read_points(e2e_gpu._h, records.ctypes.data, records.size)
+        dens = e2e_gpu.read_density()
+        t = time.perf_counter() - t0
+        if j > 0:  # the first job warms host paths
+            job_times.append(t)
+    e2e_gpu.close()
+    job = ranks.max(statistics.median(job_times))
+    e2e_value = ranks.sum(float(n) * ITERATIONS_PER_JOB) / job
+    h2d = w.xy.nbytes + w.starts.nbytes
+    d2h = records.nbytes + dens.nbytes
+
+    cpu = None
+    if ranks.rank == 0 and ranks.world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_sample(w, target_seconds=args.cpu_seconds)
+
+    per_iter = 1 + scan_launches(info.grid_width * info.fine_cells * info.grid_height * info.fine_cells) + 1 + 3
+    if (w.width * w.height) % 4:
+        per_iter += 1
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ranks.world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded random-walk polylines; reference datasets are LFS stubs)",
+        "config": {
+            "workload": "large: 100k polylines (2-8 control points), 2048^2, spacing 1/1000, sigma 16 px, radius 16",
+            "samples": n, "edges": w.edges, "grid": [w.width, w.height], "radius": w.radius, "sigma": w.sigma,
+            "search_cells_per_grid_cell": info.fine_cells, "iterations_per_job": ITERATIONS_PER_JOB,
+            "parallelism": f"replicas x{ranks.world}", "l2": "inputs larger than L2 (~330 MB working set per step)",
+        },
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                "step": f"upload + {ITERATIONS_PER_JOB} iterations + readback of records and density",
+                "seconds_per_job": job},
+        "roofline": {
+            "kernel": "neighbor_mean", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "traffic": profile_traffic(), "peak_source": peak_kind,
+            "bytes_per_launch": bytes_per_launch, "ms_per_launch": mean_ms,
+            "note": "the neighbour test is FP32-issue bound at radius 16 (~1,100 neighbours per sample)",
+        },
+        "stage_ms_per_step": {k: v / args.steps for k, v in stages.items()},
+        "stage_share": {k: v / total_stage for k, v in stages.items()} if total_stage else {},
+        "gpu_launches": per_iter * args.steps,
+        "clocks": clocks,
+        "cpu_baseline": cpu,
+    }
+    if ranks.rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse_args()
+    ranks = Ranks(args.gpus)
+    try:
+        if args.impl == "reference":
+            run_reference(args, ranks)
+        else:
+            run_ours(args, ranks)
+    finally:
+        ranks.close()
+
+
+if __name__ == "__main__":
+    main()

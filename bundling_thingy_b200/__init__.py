@@ -1,0 +1,487 @@
+"""B200-native edge bundling: Python mirror of lpstankus/bundling_thingy's API.
+
+The compute path is ``libbt.so`` (CUDA for sm_100a, C ABI in ``include/bt.h``);
+this module only binds it with ctypes. There is no CPU fallback: every call
+that computes goes through the library, and constructing a :class:`Gpu` fails
+loudly when the library or a CUDA device is missing.
+
+Names follow the reference:
+
+* :class:`Graph` — ``Graph::load/parse/normalization/points/starts``
+  (src/graph.rs).
+* :class:`Gpu` — ``Gpu::new/upload/iterate/distortion_layout/
+  distortion_snapshot`` (src/gpu.rs), plus device readbacks.
+* :class:`Layout`, :func:`squared_integral`, :class:`Aggregate` —
+  ``bundling_wgpu::geometry`` and ``bundling_wgpu::distortion``.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from dataclasses import dataclass, field
+
+import numpy as np
+
+__all__ = [
+    "BtError", "Options", "Graph", "Gpu", "Info", "Layout", "Snapshot", "Aggregate", "Measurement",
+    "squared_integral", "library", "library_path", "build", "COLOR_BY_DENSITY", "COLOR_BY_EDGE_ID", "SIZE",
+]
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = os.path.join(_HERE, "libbt.so")
+SIZE = 1600                      # headless canvas of the reference (src/gpu.rs:21)
+COLOR_BY_DENSITY = 0
+COLOR_BY_EDGE_ID = 1
+
+_f32p = ctypes.POINTER(ctypes.c_float)
+_u32p = ctypes.POINTER(ctypes.c_uint32)
+_f64p = ctypes.POINTER(ctypes.c_double)
+_vp = ctypes.c_void_p
+
+STATUS = {
+    0: "ok", 1: "capacity overflow", 2: "count/emit mismatch", 3: "invalid input", 4: "no graph",
+    5: "memory budget", 6: "timeout", 7: "CUDA error", 8: "not configured",
+}
+
+
+class BtError(RuntimeError):
+    """A non-zero bt_status with the library's message."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{message} [{STATUS.get(status, status)}]")
+        self.status = status
+        self.message = message
+
+
+class _Options(ctypes.Structure):
+    _fields_ = [
+        ("width", ctypes.c_uint32), ("height", ctypes.c_uint32), ("neighbor_radius", ctypes.c_uint32),
+        ("color_by", ctypes.c_uint32), ("max_graph_memory_bytes", ctypes.c_uint64),
+        ("evaluate_distortion", ctypes.c_uint32), ("device", ctypes.c_int32),
+        ("sample_spacing", ctypes.c_float), ("blur_sigma", ctypes.c_float), ("blur_shrink", ctypes.c_float),
+        ("fine_cells", ctypes.c_uint32), ("use_graphs", ctypes.c_uint32), ("timing", ctypes.c_uint32),
+        ("record_neighbors", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 7),
+    ]
+
+
+class _Info(ctypes.Structure):
+    _fields_ = [
+        ("samples", ctypes.c_uint32), ("paths", ctypes.c_uint32), ("drawn_paths", ctypes.c_uint32),
+        ("segments", ctypes.c_uint32), ("capacity", ctypes.c_uint32), ("iterations", ctypes.c_uint32),
+        ("grid_width", ctypes.c_uint32), ("grid_height", ctypes.c_uint32), ("fine_cells", ctypes.c_uint32),
+        ("density_passes", ctypes.c_uint32), ("device_bytes", ctypes.c_uint64), ("reserved_bytes", ctypes.c_uint64),
+    ]
+
+
+# Every entry point of include/bt.h with its ctypes signature.
+SIGNATURES = {
+    "bt_abi_version": ([], ctypes.c_int32),
+    "bt_options_init": ([ctypes.POINTER(_Options)], None),
+    "bt_create": ([ctypes.POINTER(_Options), ctypes.POINTER(_vp)], ctypes.c_int32),
+    "bt_destroy": ([_vp], None),
+    "bt_last_error": ([_vp], ctypes.c_char_p),
+    "bt_upload": ([_vp, _f32p, ctypes.c_uint32, _u32p, ctypes.c_uint32, _u32p], ctypes.c_int32),
+    "bt_upload_graph": ([_vp, _vp, _u32p], ctypes.c_int32),
+    "bt_iterate": ([_vp, ctypes.c_uint32], ctypes.c_int32),
+    "bt_iterate_async": ([_vp, ctypes.c_uint32], ctypes.c_int32),
+    "bt_synchronize": ([_vp], ctypes.c_int32),
+    "bt_iterate_timed": ([_vp, ctypes.c_uint32, _f32p], ctypes.c_int32),
+    "bt_get_info": ([_vp, ctypes.POINTER(_Info)], ctypes.c_int32),
+    "bt_read_points": ([_vp, _vp, ctypes.c_size_t], ctypes.c_int32),
+    "bt_read_paths": ([_vp, _vp, ctypes.c_size_t], ctypes.c_int32),
+    "bt_read_segments": ([_vp, _u32p, ctypes.c_size_t], ctypes.c_int32),
+    "bt_read_edges": ([_vp, _f32p, ctypes.c_size_t], ctypes.c_int32),
+    "bt_read_density": ([_vp, _f32p, ctypes.c_size_t], ctypes.c_int32),
+    "bt_read_density_raw": ([_vp, _f32p, ctypes.c_size_t, _f32p], ctypes.c_int32),
+    "bt_read_counts": ([_vp, _u32p, ctypes.c_size_t], ctypes.c_int32),
+    "bt_read_cells": ([_vp, _u32p, ctypes.c_size_t], ctypes.c_int32),
+    "bt_read_binning": ([_vp, _u32p, ctypes.c_size_t, _u32p, ctypes.c_size_t], ctypes.c_int32),
+    "bt_read_neighbors": ([_vp, _u32p, ctypes.c_size_t], ctypes.c_int32),
+    "bt_distortion": ([_vp, ctypes.c_uint32, _f64p, _f64p], ctypes.c_int32),
+    "bt_stage_times": ([_vp, ctypes.POINTER(ctypes.c_char_p), _f32p, ctypes.c_uint32, _u32p], ctypes.c_int32),
+    "bt_graph_parse": ([ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(_vp)], ctypes.c_int32),
+    "bt_graph_load": ([ctypes.c_char_p, ctypes.POINTER(_vp)], ctypes.c_int32),
+    "bt_graph_free": ([_vp], None),
+    "bt_graph_point_count": ([_vp], ctypes.c_uint32),
+    "bt_graph_start_count": ([_vp], ctypes.c_uint32),
+    "bt_graph_points": ([_vp], _f32p),
+    "bt_graph_starts": ([_vp], _u32p),
+    "bt_graph_normalization": ([_vp, _f32p], ctypes.c_int32),
+    "bt_layout_check": ([_u32p, ctypes.c_uint32, ctypes.c_uint32], ctypes.c_int32),
+    "bt_decode_points": ([_u32p, ctypes.c_uint32, ctypes.c_uint32, _vp, ctypes.c_size_t, _f32p], ctypes.c_int32),
+    "bt_squared_integral": ([_f32p, ctypes.c_size_t, _f32p, ctypes.c_size_t, _f64p], ctypes.c_int32),
+}
+
+_lib = None
+
+
+def library_path() -> str:
+    return _LIB
+
+
+def build() -> None:
+    """Compile libbt.so in-tree for sm_100a (nvcc cross-compiles without a GPU)."""
+    subprocess.run(["make", "-s", "-C", os.path.join(_HERE, "csrc"), "-j8"], check=True)
+
+
+def library():
+    """The loaded libbt.so; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB):
+            raise ImportError(f"libbt.so is missing at {_LIB}; build it with bundling_thingy_b200.build()")
+        lib = ctypes.CDLL(_LIB)
+        for name, (args, res) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.argtypes = args
+            fn.restype = res
+        _lib = lib
+    return _lib
+
+
+def _check(status: int, handle=None) -> None:
+    if status:
+        msg = library().bt_last_error(handle)
+        raise BtError(status, msg.decode() if msg else "")
+
+
+def _p(a: np.ndarray, t):
+    return a.ctypes.data_as(t)
+
+
+@dataclass
+class Options:
+    """Options of ``Gpu::new`` (src/main.rs:34-90) plus this library's extensions.
+
+    ``sample_spacing`` (fraction of the canvas; 0 = one texel), ``blur_sigma``
+    (texels; 0 = the reference's fixed sigma-6 taps) and ``blur_shrink``
+    (sigma factor per density pass) default to the reference behaviour.
+    """
+
+    width: int = SIZE
+    height: int = SIZE
+    neighbor_radius: int | None = None
+    color_by: int = COLOR_BY_DENSITY
+    max_graph_memory_mib: int = 1024
+    evaluate_distortion: bool = False
+    device: int = 0
+    sample_spacing: float = 0.0
+    blur_sigma: float = 0.0
+    blur_shrink: float = 1.0
+    fine_cells: int = 0
+    use_graphs: bool = True
+    timing: bool = False
+    record_neighbors: bool = False
+
+    def _struct(self) -> _Options:
+        o = _Options()
+        library().bt_options_init(ctypes.byref(o))
+        o.width, o.height = self.width, self.height
+        o.neighbor_radius = self.neighbor_radius or 0
+        o.color_by = self.color_by
+        o.max_graph_memory_bytes = int(self.max_graph_memory_mib) * 1024 * 1024
+        o.evaluate_distortion = int(bool(self.evaluate_distortion))
+        o.device = self.device
+        o.sample_spacing = self.sample_spacing
+        o.blur_sigma = self.blur_sigma
+        o.blur_shrink = self.blur_shrink
+        o.fine_cells = self.fine_cells
+        o.use_graphs = int(bool(self.use_graphs))
+        o.timing = int(bool(self.timing))
+        o.record_neighbors = int(bool(self.record_neighbors))
+        return o
+
+    def resample_scale(self) -> tuple[float, float]:
+        """The resampling texel_scale the library derives (resampling.wgsl:87)."""
+        if self.sample_spacing > 0:
+            s = float(np.float32(0.5 / float(np.float32(self.sample_spacing))))
+            return s, s
+        return (float(np.float32(self.width - 1) * np.float32(0.5)),
+                float(np.float32(self.height - 1) * np.float32(0.5)))
+
+
+class Graph:
+    """Parsed trail graph (src/graph.rs:7-107)."""
+
+    def __init__(self, handle):
+        self._h = handle
+
+    @classmethod
+    def parse(cls, text: str | bytes) -> "Graph":
+        data = text.encode() if isinstance(text, str) else bytes(text)
+        h = _vp()
+        _check(library().bt_graph_parse(data, len(data), ctypes.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def load(cls, path: str | os.PathLike) -> "Graph":
+        h = _vp()
+        _check(library().bt_graph_load(os.fsencode(path), ctypes.byref(h)))
+        return cls(h)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and _lib is not None:
+            _lib.bt_graph_free(h)
+            self._h = None
+
+    def points(self) -> np.ndarray:
+        n = library().bt_graph_point_count(self._h)
+        ptr = library().bt_graph_points(self._h)
+        return np.ctypeslib.as_array(ptr, shape=(n * 2,)).copy().reshape(-1, 2) if n else np.zeros((0, 2), np.float32)
+
+    def starts(self) -> np.ndarray:
+        n = library().bt_graph_start_count(self._h)
+        ptr = library().bt_graph_starts(self._h)
+        return np.ctypeslib.as_array(ptr, shape=(n,)).copy()
+
+    def normalization(self) -> np.ndarray:
+        out = np.zeros(5, np.float32)
+        _check(library().bt_graph_normalization(self._h, _p(out, _f32p)))
+        return out
+
+
+@dataclass
+class Info:
+    samples: int
+    paths: int
+    drawn_paths: int
+    segments: int
+    capacity: int
+    iterations: int
+    grid_width: int
+    grid_height: int
+    fine_cells: int
+    density_passes: int
+    device_bytes: int
+    reserved_bytes: int
+
+
+class Gpu:
+    """The reference's ``Gpu`` (src/gpu.rs:24-720), compute parts only."""
+
+    def __init__(self, options: Options | None = None):
+        self.options = options or Options()
+        h = _vp()
+        o = self.options._struct()
+        _check(library().bt_create(ctypes.byref(o), ctypes.byref(h)))
+        self._h = h
+
+    def close(self) -> None:
+        h = getattr(self, "_h", None)
+        if h and _lib is not None:
+            _lib.bt_destroy(h)
+        self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _ck(self, status: int) -> None:
+        _check(status, self._h)
+
+    # -- Gpu::upload / iterate --
+    def upload(self, graph: "Graph | tuple[np.ndarray, np.ndarray]") -> int:
+        """Gpu::upload (src/gpu.rs:493-525); returns the sample count."""
+        n = ctypes.c_uint32()
+        if isinstance(graph, Graph):
+            self._ck(library().bt_upload_graph(self._h, graph._h, ctypes.byref(n)))
+        else:
+            xy, starts = graph
+            xy = np.ascontiguousarray(xy, np.float32)
+            starts = np.ascontiguousarray(starts, np.uint32)
+            self._ck(library().bt_upload(self._h, _p(xy, _f32p), xy.size // 2, _p(starts, _u32p), starts.size,
+                                         ctypes.byref(n)))
+        return n.value
+
+    def iterate(self, n: int = 1) -> None:
+        """Gpu::iterate (src/gpu.rs:527-553), n times."""
+        self._ck(library().bt_iterate(self._h, n))
+
+    def iterate_async(self, n: int = 1) -> None:
+        self._ck(library().bt_iterate_async(self._h, n))
+
+    def iterate_timed(self, n: int = 1) -> float:
+        """Gpu::iterate n times; returns device milliseconds (CUDA events on
+        the context's stream)."""
+        ms = np.zeros(1, np.float32)
+        self._ck(library().bt_iterate_timed(self._h, n, _p(ms, _f32p)))
+        return float(ms[0])
+
+    def synchronize(self) -> None:
+        self._ck(library().bt_synchronize(self._h))
+
+    def info(self) -> Info:
+        i = _Info()
+        self._ck(library().bt_get_info(self._h, ctypes.byref(i)))
+        return Info(*(getattr(i, f) for f, _ in _Info._fields_))
+
+    # -- readbacks --
+    def read_records(self) -> np.ndarray:
+        """Raw 12-byte {x, y, edge_id} records (sample order)."""
+        n = self.info().samples
+        out = np.zeros(n * 12, np.uint8)
+        self._ck(library().bt_read_points(self._h, out.ctypes.data, out.size))
+        return out
+
+    def read_points(self) -> tuple[np.ndarray, np.ndarray]:
+        rec = self.read_records().view(np.uint32).reshape(-1, 3)
+        return rec[:, :2].copy().view(np.float32), rec[:, 2].copy()
+
+    def read_paths(self) -> np.ndarray:
+        n = self.info().paths
+        out = np.zeros((n, 3), np.uint32)
+        self._ck(library().bt_read_paths(self._h, out.ctypes.data, out.nbytes))
+        return out
+
+    def read_segments(self) -> np.ndarray:
+        n = self.info().segments
+        out = np.zeros(n, np.uint32)
+        self._ck(library().bt_read_segments(self._h, _p(out, _u32p), n))
+        return out
+
+    def read_edges(self) -> np.ndarray:
+        n = self.info().paths
+        out = np.zeros((n, 4), np.float32)
+        self._ck(library().bt_read_edges(self._h, _p(out, _f32p), out.size))
+        return out
+
+    def read_density(self) -> np.ndarray:
+        o = self.options
+        out = np.zeros(o.width * o.height, np.float32)
+        self._ck(library().bt_read_density(self._h, _p(out, _f32p), out.size))
+        return out
+
+    def read_density_raw(self) -> tuple[np.ndarray, float]:
+        o = self.options
+        out = np.zeros(o.width * o.height, np.float32)
+        peak = np.zeros(1, np.float32)
+        self._ck(library().bt_read_density_raw(self._h, _p(out, _f32p), out.size, _p(peak, _f32p)))
+        return out, float(peak[0])
+
+    def read_counts(self) -> np.ndarray:
+        o = self.options
+        out = np.zeros(o.width * o.height, np.uint32)
+        self._ck(library().bt_read_counts(self._h, _p(out, _u32p), out.size))
+        return out
+
+    def read_cells(self) -> np.ndarray:
+        out = np.zeros(self.info().samples, np.uint32)
+        self._ck(library().bt_read_cells(self._h, _p(out, _u32p), out.size))
+        return out
+
+    def read_binning(self) -> tuple[np.ndarray, np.ndarray]:
+        info = self.info()
+        k = info.fine_cells
+        cells = info.grid_width * k * info.grid_height * k
+        slots = np.zeros(info.samples, np.uint32)
+        starts = np.zeros(cells + 1, np.uint32)
+        self._ck(library().bt_read_binning(self._h, _p(slots, _u32p), slots.size, _p(starts, _u32p), starts.size))
+        return slots, starts
+
+    def read_neighbors(self) -> np.ndarray:
+        out = np.zeros(self.info().samples, np.uint32)
+        self._ck(library().bt_read_neighbors(self._h, _p(out, _u32p), out.size))
+        return out
+
+    def distortion(self, size: int = SIZE) -> "Measurement":
+        d = ctypes.c_double()
+        r = ctypes.c_double()
+        self._ck(library().bt_distortion(self._h, size, ctypes.byref(d), ctypes.byref(r)))
+        return Measurement(d.value, r.value)
+
+    def stage_times(self) -> dict[str, float]:
+        cap = 64
+        names = (ctypes.c_char_p * cap)()
+        ms = np.zeros(cap, np.float32)
+        count = ctypes.c_uint32()
+        self._ck(library().bt_stage_times(self._h, names, _p(ms, _f32p), cap, ctypes.byref(count)))
+        return {names[i].decode(): float(ms[i]) for i in range(min(count.value, cap))}
+
+    # -- distortion readback (src/gpu.rs:438-482) --
+    def distortion_layout(self) -> "Layout":
+        return Layout(self.read_paths(), self.info().samples)
+
+    def distortion_snapshot(self, layout: "Layout") -> "Snapshot":
+        return layout.decode(self.read_records())
+
+
+@dataclass
+class Measurement:
+    distortion: float
+    rms_displacement_pixels: float
+
+
+class Layout:
+    """geometry::Layout (src/geometry.rs:19-105): validated path reservations."""
+
+    def __init__(self, paths: np.ndarray, samples: int):
+        self.paths = np.ascontiguousarray(paths, np.uint32).reshape(-1, 3)
+        self.samples = int(samples)
+        _check(library().bt_layout_check(_p(self.paths, _u32p), self.paths.shape[0], self.samples))
+        counts = self.paths[:, 2]
+        order = np.argsort(self.paths[:, 0], kind="stable")
+        self.edge_ids = order[counts[order] > 0].astype(np.uint32)
+        self.skipped_count = int((counts == 0).sum())
+        self.edge_count = int(self.edge_ids.size)
+
+    def decode(self, records: np.ndarray) -> "Snapshot":
+        rec = np.ascontiguousarray(records, np.uint8)
+        xy = np.zeros((self.samples, 2), np.float32)
+        _check(library().bt_decode_points(_p(self.paths, _u32p), self.paths.shape[0], self.samples,
+                                          rec.ctypes.data, rec.size, _p(xy, _f32p)))
+        return Snapshot(self, xy)
+
+
+@dataclass
+class Snapshot:
+    """geometry::Snapshot (src/geometry.rs:190-223)."""
+
+    layout: Layout
+    positions: np.ndarray
+
+    def edges(self):
+        for e in self.layout.edge_ids:
+            off, _, cnt = self.layout.paths[e]
+            yield int(e), self.positions[off:off + cnt]
+
+
+def squared_integral(original: np.ndarray, current: np.ndarray) -> float:
+    """distortion::squared_integral (src/distortion.rs:137-168)."""
+    a = np.ascontiguousarray(original, np.float32)
+    b = np.ascontiguousarray(current, np.float32)
+    out = ctypes.c_double()
+    _check(library().bt_squared_integral(_p(a, _f32p), a.size // 2, _p(b, _f32p), b.size // 2, ctypes.byref(out)))
+    return out.value
+
+
+@dataclass
+class Aggregate:
+    """distortion::Aggregate (src/distortion.rs:172-216): equal-edge mean with
+    Kahan summation."""
+
+    value: float = 0.0
+    correction: float = 0.0
+    edges: int = 0
+
+    def add(self, original: np.ndarray, current: np.ndarray) -> None:
+        term = squared_integral(original, current)
+        adjusted = term - self.correction
+        nxt = self.value + adjusted
+        if not np.isfinite(nxt):
+            raise BtError(3, "nonfinite distortion aggregate")
+        self.correction = (nxt - self.value) - adjusted
+        self.value = nxt
+        self.edges += 1
+
+    def finish(self, size: int = SIZE) -> Measurement:
+        if self.edges == 0:
+            raise BtError(3, "distortion requires at least one edge")
+        rms = (self.value / self.edges) ** 0.5
+        return Measurement(rms / (2.0 * 2.0 ** 0.5), rms * (size / 2.0))

@@ -1,0 +1,956 @@
+// context.cu — bt_ctx (the reference's `Gpu`, src/gpu.rs) and the C ABI.
+//
+// One context = one device, one CUDA stream and the device buffers of one
+// graph. Upload and iterate enqueue the kernels of resample.cu, density.cu and
+// grid.cu on that stream; blocking calls wait with a deadline. With a constant
+// blur sigma the iteration is captured once per ping-pong parity as a CUDA
+// graph and replayed.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "bt.h"
+#include "host.h"
+#include "kernels.cuh"
+#include "scan.cuh"
+
+namespace {
+
+thread_local std::string g_thread_error;
+
+constexpr uint64_t kMiB = 1024ull * 1024ull;
+constexpr uint64_t kDistortionStagingBytes = 4194300;   // resampling.rs:16
+constexpr uint32_t kMaxDimension = 32768;
+constexpr double kWaitSeconds = 60.0;                   // gpu.rs:484-490
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    template <typename T>
+    T* as() const {
+        return static_cast<T*>(p);
+    }
+};
+
+struct StageRec {
+    const char* name;
+    cudaEvent_t start, stop;
+};
+
+}  // namespace
+
+struct bt_graph {
+    bt::HostGraph g;
+};
+
+struct bt_ctx {
+    bt_options opt{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    std::string err;
+
+    bt::Map map{};
+    bt::Grid grid{};
+    bool has_grid = false, accumulate = false;
+    float rsx = 0.f, rsy = 0.f;
+    uint64_t grid_bytes_ref = 0, staging_ref = 0;
+    size_t cells = 0, texels = 0;
+
+    DevBuf cp, starts, packed, offsets, scan64, edges, paths, totals, status;
+    DevBuf edge_ids, segments, tmp_xy, tmp_tag, tmp_cell, neighbors, baseline, current;
+    DevBuf sorted_xy[2], sorted_q[2], sorted_tag[2];
+    DevBuf hist, cell_start, scan32;
+    DevBuf counts, himg, vimg, norm, peak;
+    DevBuf records, integrals;
+    unsigned long long* h_totals = nullptr;   // pinned
+    uint32_t* h_status = nullptr;             // pinned
+    size_t device_bytes = 0;
+
+    bool uploaded = false;
+    uint32_t samples = 0, n_paths = 0, drawn = 0, capacity = 0;
+    uint64_t reserved_bytes = 0;
+    uint32_t iterations = 0, density_passes = 0;
+    int cur = 0;
+
+    cudaGraphExec_t graphs[2] = {nullptr, nullptr};
+
+    std::vector<StageRec> stage_log;
+    std::vector<StageRec> stage_pool;
+    size_t stage_used = 0;
+};
+
+namespace {
+
+bt_status fail(bt_ctx* c, bt_status code, const std::string& msg) {
+    if (c) c->err = msg;
+    g_thread_error = msg;
+    return code;
+}
+
+bt_status cuda_fail(bt_ctx* c, cudaError_t e, const char* what) {
+    const bt_status code = (e == cudaErrorMemoryAllocation) ? BT_ERR_BUDGET : BT_ERR_CUDA;
+    return fail(c, code, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define BT_CUDA(ctx, call)                                        \
+    do {                                                          \
+        cudaError_t e_ = (call);                                  \
+        if (e_ != cudaSuccess) return cuda_fail((ctx), e_, #call);\
+    } while (0)
+
+bt_status ensure(bt_ctx* c, DevBuf& b, size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    if (b.bytes >= bytes) return BT_OK;
+    if (b.p) {
+        cudaFree(b.p);
+        c->device_bytes -= b.bytes;
+        b.p = nullptr;
+        b.bytes = 0;
+    }
+    cudaError_t e = cudaMalloc(&b.p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return cuda_fail(c, e, "device allocation");
+    }
+    b.bytes = bytes;
+    c->device_bytes += bytes;
+    return BT_OK;
+}
+
+void release(DevBuf& b) {
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.bytes = 0;
+}
+
+// Blur taps for sigma (0 = the reference's fixed sigma-6 table, blur.wgsl:41-60).
+bool blur_taps(double sigma, bt::Taps* t) {
+    static const float kReference[19] = {
+        0.0666251319f, 0.0657061792f, 0.0630246744f, 0.0587964725f, 0.0533492351f,
+        0.0470805347f, 0.0404101852f, 0.0337346772f, 0.0273904106f, 0.0216300135f,
+        0.0166131238f, 0.0124102942f, 0.0090167311f, 0.0063716575f, 0.0043791719f,
+        0.0029273040f, 0.0019031803f, 0.0012034507f, 0.0007401384f};
+    std::memset(t, 0, sizeof(*t));
+    if (sigma == 0.0) {
+        for (int k = 0; k < 19; ++k) t->w[k] = kReference[k];
+        t->R = 18;
+        return true;
+    }
+    if (!(sigma > 0.0) || !std::isfinite(sigma)) return false;
+    int R = static_cast<int>(std::ceil(3.0 * sigma));
+    if (R < 1) R = 1;
+    if (R > bt::kMaxTaps - 1) return false;
+    double total = 0.0;
+    for (int k = -R; k <= R; ++k) total += std::exp(-(double)k * k / (2.0 * sigma * sigma));
+    for (int k = 0; k <= R; ++k) t->w[k] = static_cast<float>(std::exp(-(double)k * k / (2.0 * sigma * sigma)) / total);
+    t->R = R;
+    return true;
+}
+
+double sigma_for_pass(const bt_options& o, uint32_t pass) {
+    double sigma = o.blur_sigma;
+    const double shrink = (o.blur_shrink == 0.0f) ? 1.0 : static_cast<double>(o.blur_shrink);
+    for (uint32_t i = 0; i < pass && sigma != 0.0; ++i) sigma *= shrink;
+    return sigma;
+}
+
+bool constant_sigma(const bt_options& o) {
+    return o.blur_sigma == 0.0f || o.blur_shrink == 0.0f || o.blur_shrink == 1.0f;
+}
+
+// GridParameters (neighbor_mean.rs:26-46) byte accounting of the reference.
+uint64_t reference_grid_bytes(uint32_t w, uint32_t h, uint32_t r) {
+    const uint64_t cells = static_cast<uint64_t>((w + r - 1) / r) * ((h + r - 1) / r);
+    return cells * 8 + 8 + cells * 24 + 52;
+}
+
+// Stage timing (GpuTimings, src/profiling.rs:35-136).
+void stage_begin(bt_ctx* c, const char* name) {
+    if (!c->opt.timing) return;
+    if (c->stage_used == c->stage_pool.size()) {
+        StageRec r{name, nullptr, nullptr};
+        cudaEventCreate(&r.start);
+        cudaEventCreate(&r.stop);
+        c->stage_pool.push_back(r);
+    }
+    StageRec& r = c->stage_pool[c->stage_used++];
+    r.name = name;
+    cudaEventRecord(r.start, c->stream);
+}
+
+void stage_end(bt_ctx* c) {
+    if (!c->opt.timing || c->stage_used == 0) return;
+    cudaEventRecord(c->stage_pool[c->stage_used - 1].stop, c->stream);
+}
+
+bt_status wait(bt_ctx* c) {
+    cudaError_t e = cudaEventRecord(c->done, c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "cudaEventRecord");
+    const auto start = std::chrono::steady_clock::now();
+    int spins = 0;
+    while (true) {
+        e = cudaEventQuery(c->done);
+        if (e == cudaSuccess) break;
+        if (e != cudaErrorNotReady) return cuda_fail(c, e, "device execution");
+        const double waited = std::chrono::duration<double>(std::chrono::steady_clock::now() - start).count();
+        if (waited > kWaitSeconds) return fail(c, BT_ERR_TIMEOUT, "device wait exceeded 60 s");
+        if (++spins < 2000) {
+            std::this_thread::yield();
+        } else {
+            std::this_thread::sleep_for(std::chrono::microseconds(50));
+        }
+    }
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(c, e, "kernel launch");
+    return BT_OK;
+}
+
+void drop_graphs(bt_ctx* c) {
+    for (auto& g : c->graphs) {
+        if (g) cudaGraphExecDestroy(g);
+        g = nullptr;
+    }
+}
+
+// Density::encode (density.rs:155-166) for density pass `pass`.
+bt_status enqueue_density(bt_ctx* c, uint32_t pass) {
+    bt::Taps taps;
+    if (!blur_taps(sigma_for_pass(c->opt, pass), &taps)) return fail(c, BT_ERR_INVALID, "invalid blur sigma");
+    stage_begin(c, "density.blur_horizontal");
+    bt::launch_blur_horizontal(c->counts.as<uint32_t>(), c->himg.as<float>(), c->map.w, c->map.h, taps, c->stream);
+    stage_end(c);
+    stage_begin(c, "density.blur_vertical_and_maximum");
+    bt::launch_blur_vertical(c->himg.as<float>(), c->vimg.as<float>(), c->map.w, c->map.h, taps,
+                             c->peak.as<uint32_t>(), c->stream);
+    stage_end(c);
+    stage_begin(c, "density.normalize");
+    bt::launch_normalize(c->vimg.as<float>(), c->peak.as<uint32_t>(), c->norm.as<float>(), c->texels, c->stream);
+    stage_end(c);
+    return BT_OK;
+}
+
+// Scan of the search-cell populations and the scatter into slot order `dst`.
+void enqueue_binning(bt_ctx* c, int dst) {
+    stage_begin(c, "graph.grid_scan");
+    bt::exclusive_scan<uint32_t>(c->hist.as<uint32_t>(), c->cell_start.as<uint32_t>(), c->cells,
+                                 c->scan32.as<uint32_t>(), c->stream);
+    stage_end(c);
+    stage_begin(c, "graph.grid_scatter");
+    bt::ScatterArgs s{};
+    s.xy = c->tmp_xy.as<float2>();
+    s.tag = c->tmp_tag.as<uint32_t>();
+    s.cell = c->tmp_cell.as<uint32_t>();
+    s.cell_start = c->cell_start.as<uint32_t>();
+    s.hist = c->hist.as<uint32_t>();
+    s.out_xy = c->sorted_xy[dst].as<float2>();
+    s.out_q = c->sorted_q[dst].as<int2>();
+    s.out_tag = c->sorted_tag[dst].as<uint32_t>();
+    s.n = c->samples;
+    s.cells = static_cast<uint32_t>(c->cells);
+    s.status = c->status.as<uint32_t>();
+    bt::launch_scatter(s, c->stream);
+    stage_end(c);
+}
+
+// One Gpu::iterate (gpu.rs:527-553) starting from slot order `src`.
+bt_status enqueue_iteration(bt_ctx* c, int src, uint32_t pass) {
+    if (c->accumulate) {
+        cudaMemsetAsync(c->counts.p, 0, c->texels * sizeof(uint32_t), c->stream);
+        cudaMemsetAsync(c->peak.p, 0, sizeof(uint32_t), c->stream);
+    }
+    stage_begin(c, "graph.neighbor_mean");
+    bt::MeanArgs m{};
+    m.xy = c->sorted_xy[src].as<float2>();
+    m.q = c->sorted_q[src].as<int2>();
+    m.tag = c->sorted_tag[src].as<uint32_t>();
+    m.cell_start = c->cell_start.as<uint32_t>();
+    m.out_xy = c->tmp_xy.as<float2>();
+    m.out_tag = c->tmp_tag.as<uint32_t>();
+    m.out_cell = c->tmp_cell.as<uint32_t>();
+    m.hist = c->hist.as<uint32_t>();
+    m.counts = c->accumulate ? c->counts.as<uint32_t>() : nullptr;
+    m.neighbors = c->opt.record_neighbors ? c->neighbors.as<uint32_t>() : nullptr;
+    m.n = c->samples;
+    m.g = c->grid;
+    bt::launch_neighbor_mean(m, c->stream);
+    stage_end(c);
+    enqueue_binning(c, src ^ 1);
+    if (c->accumulate) return enqueue_density(c, pass);
+    return BT_OK;
+}
+
+bt_status validate_options(const bt_options* o, bt_ctx* c) {
+    if (o->width == 0 || o->height == 0) return fail(c, BT_ERR_INVALID, "density map dimensions must be nonzero");
+    if (o->width > kMaxDimension || o->height > kMaxDimension)
+        return fail(c, BT_ERR_INVALID, "density map exceeds GPU texture limits");
+    if (o->max_graph_memory_bytes == 0) return fail(c, BT_ERR_INVALID, "graph memory budget must be nonzero");
+    if (o->color_by > BT_COLOR_BY_EDGE_ID) return fail(c, BT_ERR_INVALID, "unknown color_by");
+    if (!(o->blur_sigma >= 0.0f) || !std::isfinite(o->blur_sigma) || !(o->blur_shrink >= 0.0f) ||
+        !std::isfinite(o->blur_shrink))
+        return fail(c, BT_ERR_INVALID, "invalid blur sigma or shrink");
+    bt::Taps t;
+    if (!blur_taps(o->blur_sigma, &t)) return fail(c, BT_ERR_INVALID, "blur sigma above 42.6 texels (128 taps)");
+    if (!(o->sample_spacing >= 0.0f) || !std::isfinite(o->sample_spacing))
+        return fail(c, BT_ERR_INVALID, "invalid sample spacing");
+    if (o->sample_spacing > 0.0f && !std::isfinite(0.5 / static_cast<double>(o->sample_spacing)))
+        return fail(c, BT_ERR_INVALID, "invalid sample spacing");
+    if (o->neighbor_radius > 0 && o->fine_cells > 4096) return fail(c, BT_ERR_INVALID, "fine_cells too large");
+    const uint64_t grid = o->neighbor_radius ? reference_grid_bytes(o->width, o->height, o->neighbor_radius) : 0;
+    const uint64_t staging = o->evaluate_distortion ? kDistortionStagingBytes : 0;
+    // resampling.rs:85-89
+    if (!(grid + staging < o->max_graph_memory_bytes))
+        return fail(c, BT_ERR_BUDGET,
+                    "neighbor grid and optional distortion staging exceed --max-graph-memory-mib; increase the "
+                    "budget or --neighbor-radius");
+    return BT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t bt_abi_version(void) { return BT_ABI_VERSION; }
+
+void bt_options_init(bt_options* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->width = 1600;   // gpu.rs:21 (headless SIZE)
+    o->height = 1600;
+    o->color_by = BT_COLOR_BY_DENSITY;
+    o->max_graph_memory_bytes = 1024 * kMiB;   // main.rs:87-89
+    o->use_graphs = 1;
+}
+
+const char* bt_last_error(const bt_ctx* ctx) { return ctx ? ctx->err.c_str() : g_thread_error.c_str(); }
+
+bt_status bt_create(const bt_options* options, bt_ctx** out) {
+    if (!options || !out) return fail(nullptr, BT_ERR_INVALID, "null argument");
+    *out = nullptr;
+    if (bt_status s = validate_options(options, nullptr)) return s;
+    auto* c = new bt_ctx();
+    c->opt = *options;
+    c->device = options->device;
+    auto bail = [&](bt_status s) {
+        std::string msg = c->err;
+        bt_destroy(c);
+        g_thread_error = msg;
+        return s;
+    };
+    cudaError_t e = cudaSetDevice(c->device);
+    if (e != cudaSuccess) return bail(cuda_fail(c, e, "cudaSetDevice"));
+    if ((e = bt::prepare_density_kernels()) != cudaSuccess) return bail(cuda_fail(c, e, "kernel attributes"));
+    if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess)
+        return bail(cuda_fail(c, e, "cudaStreamCreate"));
+    if ((e = cudaEventCreateWithFlags(&c->done, cudaEventDisableTiming)) != cudaSuccess)
+        return bail(cuda_fail(c, e, "cudaEventCreate"));
+    if ((e = cudaMallocHost(&c->h_totals, 4 * sizeof(unsigned long long))) != cudaSuccess)
+        return bail(cuda_fail(c, e, "cudaMallocHost"));
+    if ((e = cudaMallocHost(&c->h_status, 4 * sizeof(uint32_t))) != cudaSuccess)
+        return bail(cuda_fail(c, e, "cudaMallocHost"));
+
+    const uint32_t W = options->width, H = options->height;
+    c->map = bt::Map{W, H, static_cast<float>(W - 1u), static_cast<float>(H - 1u)};
+    c->texels = static_cast<size_t>(W) * H;
+    c->accumulate = options->color_by == BT_COLOR_BY_DENSITY;
+    if (options->sample_spacing > 0.0f) {
+        c->rsx = c->rsy = static_cast<float>(0.5 / static_cast<double>(options->sample_spacing));
+    } else {
+        // texel_scale of resampling.wgsl:87
+        c->rsx = static_cast<float>(W - 1u) * 0.5f;
+        c->rsy = static_cast<float>(H - 1u) * 0.5f;
+    }
+    c->staging_ref = options->evaluate_distortion ? kDistortionStagingBytes : 0;
+    const uint32_t r = options->neighbor_radius;
+    c->has_grid = r > 0;
+    if (c->has_grid) {
+        bt::Grid& g = c->grid;
+        g.map = c->map;
+        g.radius = r;
+        g.rf = static_cast<float>(r);
+        g.gw = (W + r - 1) / r;
+        g.gh = (H + r - 1) / r;
+        g.k = options->fine_cells ? options->fine_cells : r;   // search cells of about one texel
+        g.inv_s = static_cast<float>(g.k) / g.rf;
+        g.s = g.rf / static_cast<float>(g.k);
+        g.fw = g.gw * g.k;
+        g.fh = g.gh * g.k;
+        g.tsx = static_cast<float>(W - 1u) * 0.5f;
+        g.tsy = static_cast<float>(H - 1u) * 0.5f;
+        g.r2 = g.rf * g.rf;
+        g.reachx = g.rf + static_cast<float>(W) * 0.00000024f;
+        g.reachy = g.rf + static_cast<float>(H) * 0.00000024f;
+        g.margin = 1e-3f + 1e-6f * static_cast<float>(std::max(W, H)) + 1e-5f * g.rf;
+        c->cells = static_cast<size_t>(g.fw) * g.fh;
+        if (c->cells > 0x7FFFFFFFull) return bail(fail(c, BT_ERR_INVALID, "neighbour search grid too large"));
+        c->grid_bytes_ref = reference_grid_bytes(W, H, r);
+        if (bt_status s = ensure(c, c->hist, c->cells * 4)) return bail(s);
+        if (bt_status s = ensure(c, c->cell_start, (c->cells + 1) * 4)) return bail(s);
+        if (bt_status s = ensure(c, c->scan32, bt::scan_scratch_elems(c->cells) * 4)) return bail(s);
+        if ((e = cudaMemsetAsync(c->hist.p, 0, c->cells * 4, c->stream)) != cudaSuccess)
+            return bail(cuda_fail(c, e, "cudaMemset"));
+    }
+    if (bt_status s = ensure(c, c->counts, c->texels * 4)) return bail(s);
+    if (bt_status s = ensure(c, c->himg, c->texels * 4)) return bail(s);
+    if (bt_status s = ensure(c, c->vimg, c->texels * 4)) return bail(s);
+    if (bt_status s = ensure(c, c->norm, c->texels * 4)) return bail(s);
+    if (bt_status s = ensure(c, c->peak, 16)) return bail(s);
+    if (bt_status s = ensure(c, c->totals, 32)) return bail(s);
+    if (bt_status s = ensure(c, c->status, 16)) return bail(s);
+    cudaMemsetAsync(c->counts.p, 0, c->texels * 4, c->stream);
+    cudaMemsetAsync(c->vimg.p, 0, c->texels * 4, c->stream);
+    cudaMemsetAsync(c->norm.p, 0, c->texels * 4, c->stream);
+    cudaMemsetAsync(c->peak.p, 0, 16, c->stream);
+    if (bt_status s = wait(c)) return bail(s);
+    *out = c;
+    return BT_OK;
+}
+
+void bt_destroy(bt_ctx* c) {
+    if (!c) return;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    drop_graphs(c);
+    DevBuf* bufs[] = {&c->cp, &c->starts, &c->packed, &c->offsets, &c->scan64, &c->edges, &c->paths, &c->totals,
+                      &c->status, &c->edge_ids, &c->segments, &c->tmp_xy, &c->tmp_tag, &c->tmp_cell,
+                      &c->neighbors, &c->baseline, &c->current, &c->sorted_xy[0], &c->sorted_xy[1],
+                      &c->sorted_q[0], &c->sorted_q[1], &c->sorted_tag[0], &c->sorted_tag[1], &c->hist,
+                      &c->cell_start, &c->scan32, &c->counts, &c->himg, &c->vimg, &c->norm, &c->peak,
+                      &c->records, &c->integrals};
+    for (DevBuf* b : bufs) release(*b);
+    for (StageRec& r : c->stage_pool) {
+        cudaEventDestroy(r.start);
+        cudaEventDestroy(r.stop);
+    }
+    if (c->h_totals) cudaFreeHost(c->h_totals);
+    if (c->h_status) cudaFreeHost(c->h_status);
+    if (c->done) cudaEventDestroy(c->done);
+    if (c->t0) cudaEventDestroy(c->t0);
+    if (c->t1) cudaEventDestroy(c->t1);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+bt_status bt_upload(bt_ctx* c, const float* xy, uint32_t n_points, const uint32_t* starts, uint32_t n_starts,
+                    uint32_t* out_samples) {
+    if (!c) return fail(nullptr, BT_ERR_INVALID, "null context");
+    if (!xy || !starts || !out_samples) return fail(c, BT_ERR_INVALID, "null argument");
+    cudaSetDevice(c->device);
+    // The previous graph is released first (gpu.rs:494-497).
+    c->uploaded = false;
+    c->samples = 0;
+    c->iterations = 0;
+    c->density_passes = 0;
+    drop_graphs(c);
+    c->stage_used = 0;
+    // Input contract of Graph (graph.rs:7-12, 60-77).
+    if (n_starts < 2 || starts[0] != 0 || starts[n_starts - 1] != n_points)
+        return fail(c, BT_ERR_INVALID, "path starts must begin at 0 and end at the point count");
+    for (uint32_t e = 0; e + 1 < n_starts; ++e)
+        if (starts[e + 1] < starts[e] || starts[e + 1] - starts[e] < 2)
+            return fail(c, BT_ERR_INVALID, "every edge needs at least two control points");
+    float mn[2] = {3.40282347e+38f, 3.40282347e+38f}, mx[2] = {-3.40282347e+38f, -3.40282347e+38f};
+    for (uint32_t i = 0; i < n_points; ++i) {
+        const float x = xy[2 * i], y = xy[2 * i + 1];
+        if (!std::isfinite(x) || !std::isfinite(y)) return fail(c, BT_ERR_INVALID, "non-finite TRL coordinate");
+        mn[0] = std::fmin(mn[0], x);
+        mn[1] = std::fmin(mn[1], y);
+        mx[0] = std::fmax(mx[0], x);
+        mx[1] = std::fmax(mx[1], y);
+    }
+    float nm[5];
+    std::string err;
+    if (!bt::normalization(mn, mx, nm, &err)) return fail(c, BT_ERR_INVALID, err);
+    const uint32_t E = n_starts - 1;
+
+    // Allocation::new (resampling.rs:321-397): capacity from the budget.
+    const uint64_t sample_bytes = 16 + (c->has_grid ? 32 : 0);
+    const uint64_t fixed = 8ull * n_points + 4ull * n_starts + 12ull * E + 16ull * E + 8ull * E + 32 + 16 + 48 + 16 +
+                           c->grid_bytes_ref + c->staging_ref;
+    if (fixed > c->opt.max_graph_memory_bytes)
+        return fail(c, BT_ERR_BUDGET,
+                    "control points, path metadata, and neighbor grid exceed --max-graph-memory-mib");
+    const uint64_t available = c->opt.max_graph_memory_bytes - fixed;
+    const uint64_t binding_limit = 0xFFFFFFFFull;   // u32-indexed storage bindings
+    uint64_t capacity = std::min(available / sample_bytes, binding_limit / 12);
+    capacity = std::min<uint64_t>(capacity, 0x7FFFFFFFull);   // sample index + movable bit in 32 bits
+    if (capacity < 3) return fail(c, BT_ERR_BUDGET, "graph memory budget has no room for resampled geometry");
+    c->capacity = static_cast<uint32_t>(capacity);
+    c->reserved_bytes = fixed + capacity * sample_bytes;
+
+    if (bt_status s = ensure(c, c->cp, 8ull * n_points)) return s;
+    if (bt_status s = ensure(c, c->starts, 4ull * n_starts)) return s;
+    if (bt_status s = ensure(c, c->packed, 8ull * E)) return s;
+    if (bt_status s = ensure(c, c->offsets, 8ull * (E + 1))) return s;
+    if (bt_status s = ensure(c, c->scan64, 8ull * bt::scan_scratch_elems(E))) return s;
+    if (bt_status s = ensure(c, c->edges, 16ull * E)) return s;
+    if (bt_status s = ensure(c, c->paths, 12ull * E)) return s;
+    BT_CUDA(c, cudaMemcpyAsync(c->cp.p, xy, 8ull * n_points, cudaMemcpyHostToDevice, c->stream));
+    BT_CUDA(c, cudaMemcpyAsync(c->starts.p, starts, 4ull * n_starts, cudaMemcpyHostToDevice, c->stream));
+    BT_CUDA(c, cudaMemsetAsync(c->totals.p, 0, 32, c->stream));
+    BT_CUDA(c, cudaMemsetAsync(c->status.p, 0, 16, c->stream));
+
+    const bt::Norm norm{nm[0], nm[1], nm[2], nm[3], nm[4]};
+    stage_begin(c, "graph.count");
+    bt::ResampleCountArgs ca{};
+    ca.cp = c->cp.as<float2>();
+    ca.starts = c->starts.as<uint32_t>();
+    ca.paths = E;
+    ca.norm = norm;
+    ca.sx = c->rsx;
+    ca.sy = c->rsy;
+    ca.capacity = c->capacity;
+    ca.packed = c->packed.as<unsigned long long>();
+    ca.edges = c->edges.as<float4>();
+    ca.totals = c->totals.as<unsigned long long>();
+    bt::launch_resample_count(ca, c->stream);
+    stage_end(c);
+    BT_CUDA(c, cudaMemcpyAsync(c->h_totals, c->totals.p, 16, cudaMemcpyDeviceToHost, c->stream));
+    if (bt_status s = wait(c)) return s;
+    const unsigned long long total = c->h_totals[0], drawn = c->h_totals[1];
+    // count_paths overflow 1 (resampling.wgsl:151-156), PendingGraph::finish (resampling.rs:294-308).
+    if (total > c->capacity)
+        return fail(c, BT_ERR_CAPACITY,
+                    "GPU resampling exceeds the " + std::to_string(c->capacity) +
+                        "-sample buffer capacity; increase --max-graph-memory-mib or reduce the graph or render "
+                        "dimensions");
+    if (total - drawn == 0) return fail(c, BT_ERR_INVALID, "resampled graph has no drawable edges");
+    const uint32_t N = static_cast<uint32_t>(total);
+    const uint32_t segs = static_cast<uint32_t>(total - drawn);
+
+    stage_begin(c, "graph.emit");
+    bt::exclusive_scan<unsigned long long>(c->packed.as<unsigned long long>(), c->offsets.as<unsigned long long>(), E,
+                                           c->scan64.as<unsigned long long>(), c->stream);
+    bt::launch_paths_from_scan(c->packed.as<unsigned long long>(), c->offsets.as<unsigned long long>(), E,
+                               c->paths.as<bt::PathRec>(), c->stream);
+    if (bt_status s = ensure(c, c->edge_ids, 4ull * N)) return s;
+    if (bt_status s = ensure(c, c->segments, 4ull * segs)) return s;
+    if (bt_status s = ensure(c, c->tmp_xy, 8ull * N)) return s;
+    if (bt_status s = ensure(c, c->tmp_tag, 4ull * N)) return s;
+    if (bt_status s = ensure(c, c->tmp_cell, 4ull * N)) return s;
+    if (c->has_grid) {
+        for (int b = 0; b < 2; ++b) {
+            if (bt_status s = ensure(c, c->sorted_xy[b], 8ull * N)) return s;
+            if (bt_status s = ensure(c, c->sorted_q[b], 8ull * N)) return s;
+            if (bt_status s = ensure(c, c->sorted_tag[b], 4ull * N)) return s;
+        }
+        if (c->opt.record_neighbors)
+            if (bt_status s = ensure(c, c->neighbors, 4ull * N)) return s;
+        BT_CUDA(c, cudaMemsetAsync(c->hist.p, 0, c->cells * 4, c->stream));
+    }
+    if (c->opt.evaluate_distortion)
+        if (bt_status s = ensure(c, c->baseline, 8ull * N)) return s;
+    if (c->accumulate) {
+        BT_CUDA(c, cudaMemsetAsync(c->counts.p, 0, c->texels * 4, c->stream));
+        BT_CUDA(c, cudaMemsetAsync(c->peak.p, 0, 4, c->stream));
+    }
+    bt::ResampleEmitArgs ea{};
+    ea.cp = c->cp.as<float2>();
+    ea.starts = c->starts.as<uint32_t>();
+    ea.paths = c->paths.as<bt::PathRec>();
+    ea.n_paths = E;
+    ea.norm = norm;
+    ea.sx = c->rsx;
+    ea.sy = c->rsy;
+    ea.map = c->map;
+    ea.xy = c->tmp_xy.as<float2>();
+    ea.edge_ids = c->edge_ids.as<uint32_t>();
+    ea.segments = c->segments.as<uint32_t>();
+    ea.counts = c->accumulate ? c->counts.as<uint32_t>() : nullptr;
+    ea.grid_host = c->has_grid ? &c->grid : nullptr;
+    ea.tag = c->tmp_tag.as<uint32_t>();
+    ea.cell = c->tmp_cell.as<uint32_t>();
+    ea.hist = c->hist.as<uint32_t>();
+    ea.status = c->status.as<uint32_t>();
+    bt::launch_resample_emit(ea, c->stream);
+    stage_end(c);
+    c->samples = N;
+    c->n_paths = E;
+    c->drawn = static_cast<uint32_t>(drawn);
+    if (c->opt.evaluate_distortion)
+        BT_CUDA(c, cudaMemcpyAsync(c->baseline.p, c->tmp_xy.p, 8ull * N, cudaMemcpyDeviceToDevice, c->stream));
+    if (c->accumulate) {
+        if (bt_status s = enqueue_density(c, 0)) return s;
+        c->density_passes = 1;
+    }
+    if (c->has_grid) {
+        enqueue_binning(c, 0);
+        c->cur = 0;
+    }
+    BT_CUDA(c, cudaMemcpyAsync(c->h_status, c->status.p, 4, cudaMemcpyDeviceToHost, c->stream));
+    if (bt_status s = wait(c)) return s;
+    if (c->h_status[0] & 2u) return fail(c, BT_ERR_MISMATCH, "GPU resampling count and write passes disagree");
+    if (c->h_status[0] & 8u) return fail(c, BT_ERR_CUDA, "inconsistent neighbour-grid binning");
+    c->uploaded = true;
+    *out_samples = N;
+    return BT_OK;
+}
+
+bt_status bt_upload_graph(bt_ctx* c, const bt_graph* g, uint32_t* out_samples) {
+    if (!g) return fail(c, BT_ERR_INVALID, "null graph");
+    return bt_upload(c, g->g.xy.data(), static_cast<uint32_t>(g->g.xy.size() / 2), g->g.starts.data(),
+                     static_cast<uint32_t>(g->g.starts.size()), out_samples);
+}
+
+bt_status bt_iterate_async(bt_ctx* c, uint32_t n) {
+    if (!c) return fail(nullptr, BT_ERR_INVALID, "null context");
+    if (!c->has_grid) return fail(c, BT_ERR_NOT_CONFIGURED, "neighbor radius is not configured");
+    if (!c->uploaded) return fail(c, BT_ERR_NO_GRAPH, "no uploaded graph");
+    cudaSetDevice(c->device);
+    c->stage_used = 0;
+    const bool use_graphs = c->opt.use_graphs && !c->opt.timing && constant_sigma(c->opt);
+    for (uint32_t i = 0; i < n; ++i) {
+        const uint32_t pass = c->density_passes;
+        if (use_graphs) {
+            cudaGraphExec_t& exec = c->graphs[c->cur];
+            if (!exec) {
+                cudaGraph_t graph = nullptr;
+                BT_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+                bt_status s = enqueue_iteration(c, c->cur, pass);
+                cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
+                if (s) {
+                    if (graph) cudaGraphDestroy(graph);
+                    return s;
+                }
+                if (e != cudaSuccess) return cuda_fail(c, e, "cudaStreamEndCapture");
+                e = cudaGraphInstantiate(&exec, graph, 0);
+                cudaGraphDestroy(graph);
+                if (e != cudaSuccess) {
+                    exec = nullptr;
+                    return cuda_fail(c, e, "cudaGraphInstantiate");
+                }
+            }
+            BT_CUDA(c, cudaGraphLaunch(exec, c->stream));
+        } else {
+            if (bt_status s = enqueue_iteration(c, c->cur, pass)) return s;
+        }
+        c->cur ^= 1;
+        c->iterations++;
+        if (c->accumulate) c->density_passes++;
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(c, e, "kernel launch");
+    return BT_OK;
+}
+
+bt_status bt_synchronize(bt_ctx* c) {
+    if (!c) return fail(nullptr, BT_ERR_INVALID, "null context");
+    cudaSetDevice(c->device);
+    return wait(c);
+}
+
+namespace {
+// Device status word after iterations (scatter guard, bit 3).
+bt_status check_iteration_status(bt_ctx* c) {
+    BT_CUDA(c, cudaMemcpyAsync(c->h_status, c->status.p, 4, cudaMemcpyDeviceToHost, c->stream));
+    if (bt_status s = wait(c)) return s;
+    if (c->h_status[0] & 8u) {
+        c->uploaded = false;
+        return fail(c, BT_ERR_CUDA, "inconsistent neighbour-grid binning");
+    }
+    return BT_OK;
+}
+}  // namespace
+
+bt_status bt_iterate(bt_ctx* c, uint32_t n) {
+    if (bt_status s = bt_iterate_async(c, n)) return s;
+    return check_iteration_status(c);
+}
+
+bt_status bt_iterate_timed(bt_ctx* c, uint32_t n, float* device_ms) {
+    if (!c || !device_ms) return fail(c, BT_ERR_INVALID, "null argument");
+    cudaSetDevice(c->device);
+    if (!c->t0) {
+        BT_CUDA(c, cudaEventCreate(&c->t0));
+        BT_CUDA(c, cudaEventCreate(&c->t1));
+    }
+    BT_CUDA(c, cudaEventRecord(c->t0, c->stream));
+    if (bt_status s = bt_iterate_async(c, n)) return s;
+    BT_CUDA(c, cudaEventRecord(c->t1, c->stream));
+    if (bt_status s = wait(c)) return s;
+    BT_CUDA(c, cudaEventElapsedTime(device_ms, c->t0, c->t1));
+    return check_iteration_status(c);
+}
+
+bt_status bt_get_info(bt_ctx* c, bt_info* info) {
+    if (!c || !info) return fail(c, BT_ERR_INVALID, "null argument");
+    std::memset(info, 0, sizeof(*info));
+    info->samples = c->samples;
+    info->paths = c->n_paths;
+    info->drawn_paths = c->drawn;
+    info->segments = c->samples ? c->samples - c->drawn : 0;
+    info->capacity = c->capacity;
+    info->iterations = c->iterations;
+    info->grid_width = c->has_grid ? c->grid.gw : 0;
+    info->grid_height = c->has_grid ? c->grid.gh : 0;
+    info->fine_cells = c->has_grid ? c->grid.k : 0;
+    info->density_passes = c->density_passes;
+    info->device_bytes = c->device_bytes;
+    info->reserved_bytes = c->reserved_bytes;
+    return BT_OK;
+}
+
+namespace {
+
+bt_status need_graph(bt_ctx* c) {
+    if (!c) return fail(nullptr, BT_ERR_INVALID, "null context");
+    if (!c->uploaded) return fail(c, BT_ERR_NO_GRAPH, "no uploaded graph");
+    cudaSetDevice(c->device);
+    return BT_OK;
+}
+
+bt_status copy_out(bt_ctx* c, void* dst, const void* src, size_t bytes) {
+    BT_CUDA(c, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c->stream));
+    return wait(c);
+}
+
+// Current positions in sample order (device buffer).
+bt_status current_positions(bt_ctx* c, const float2** out) {
+    if (!c->has_grid) {
+        *out = c->tmp_xy.as<float2>();
+        return BT_OK;
+    }
+    if (bt_status s = ensure(c, c->current, 8ull * c->samples)) return s;
+    bt::launch_positions_from_slots(c->sorted_xy[c->cur].as<float2>(), c->sorted_tag[c->cur].as<uint32_t>(),
+                                    c->samples, c->current.as<float2>(), c->stream);
+    *out = c->current.as<float2>();
+    return BT_OK;
+}
+
+}  // namespace
+
+bt_status bt_read_points(bt_ctx* c, void* dst, size_t bytes) {
+    if (bt_status s = need_graph(c)) return s;
+    if (!dst || bytes != 12ull * c->samples) return fail(c, BT_ERR_INVALID, "point buffer must hold 12 bytes per sample");
+    if (bt_status s = ensure(c, c->records, 12ull * c->samples)) return s;
+    if (c->has_grid) {
+        bt::launch_unsort_records(c->sorted_xy[c->cur].as<float2>(), c->sorted_tag[c->cur].as<uint32_t>(),
+                                  c->edge_ids.as<uint32_t>(), c->samples, c->records.as<uint32_t>(), c->stream);
+    } else {
+        bt::launch_records_from_sample_order(c->tmp_xy.as<float2>(), c->edge_ids.as<uint32_t>(), c->samples,
+                                             c->records.as<uint32_t>(), c->stream);
+    }
+    return copy_out(c, dst, c->records.p, bytes);
+}
+
+bt_status bt_read_paths(bt_ctx* c, void* dst, size_t bytes) {
+    if (bt_status s = need_graph(c)) return s;
+    if (!dst || bytes != 12ull * c->n_paths) return fail(c, BT_ERR_INVALID, "path buffer must hold 12 bytes per edge");
+    return copy_out(c, dst, c->paths.p, bytes);
+}
+
+bt_status bt_read_segments(bt_ctx* c, uint32_t* dst, size_t count) {
+    if (bt_status s = need_graph(c)) return s;
+    if (!dst || count != c->samples - c->drawn) return fail(c, BT_ERR_INVALID, "segment buffer size");
+    return copy_out(c, dst, c->segments.p, 4 * count);
+}
+
+bt_status bt_read_edges(bt_ctx* c, float* dst, size_t count) {
+    if (bt_status s = need_graph(c)) return s;
+    if (!dst || count != 4ull * c->n_paths) return fail(c, BT_ERR_INVALID, "edge buffer must hold 4 floats per edge");
+    return copy_out(c, dst, c->edges.p, 4 * count);
+}
+
+bt_status bt_read_density(bt_ctx* c, float* dst, size_t count) {
+    if (bt_status s = need_graph(c)) return s;
+    if (!c->accumulate) return fail(c, BT_ERR_NOT_CONFIGURED, "density is only accumulated when coloring by density");
+    if (!dst || count != c->texels) return fail(c, BT_ERR_INVALID, "density buffer must hold width*height floats");
+    return copy_out(c, dst, c->norm.p, 4 * count);
+}
+
+bt_status bt_read_density_raw(bt_ctx* c, float* dst, size_t count, float* peak) {
+    if (bt_status s = need_graph(c)) return s;
+    if (!c->accumulate) return fail(c, BT_ERR_NOT_CONFIGURED, "density is only accumulated when coloring by density");
+    if (!dst || !peak || count != c->texels) return fail(c, BT_ERR_INVALID, "density buffer size");
+    BT_CUDA(c, cudaMemcpyAsync(dst, c->vimg.p, 4 * count, cudaMemcpyDeviceToHost, c->stream));
+    uint32_t bits = 0;
+    BT_CUDA(c, cudaMemcpyAsync(c->h_status + 1, c->peak.p, 4, cudaMemcpyDeviceToHost, c->stream));
+    if (bt_status s = wait(c)) return s;
+    bits = c->h_status[1];
+    std::memcpy(peak, &bits, 4);
+    return BT_OK;
+}
+
+bt_status bt_read_counts(bt_ctx* c, uint32_t* dst, size_t count) {
+    if (bt_status s = need_graph(c)) return s;
+    if (!c->accumulate) return fail(c, BT_ERR_NOT_CONFIGURED, "density is only accumulated when coloring by density");
+    if (!dst || count != c->texels) return fail(c, BT_ERR_INVALID, "count buffer must hold width*height values");
+    return copy_out(c, dst, c->counts.p, 4 * count);
+}
+
+bt_status bt_read_cells(bt_ctx* c, uint32_t* dst, size_t count) {
+    if (bt_status s = need_graph(c)) return s;
+    if (!c->has_grid) return fail(c, BT_ERR_NOT_CONFIGURED, "neighbor radius is not configured");
+    if (!dst || count != c->samples) return fail(c, BT_ERR_INVALID, "cell buffer must hold one id per sample");
+    if (bt_status s = ensure(c, c->records, 12ull * c->samples)) return s;
+    bt::launch_grid_cells(c->sorted_xy[c->cur].as<float2>(), c->sorted_tag[c->cur].as<uint32_t>(), c->samples,
+                          c->grid, c->records.as<uint32_t>(), c->stream);
+    return copy_out(c, dst, c->records.p, 4 * count);
+}
+
+bt_status bt_read_binning(bt_ctx* c, uint32_t* slot_samples, size_t count, uint32_t* cell_starts, size_t cell_count) {
+    if (bt_status s = need_graph(c)) return s;
+    if (!c->has_grid) return fail(c, BT_ERR_NOT_CONFIGURED, "neighbor radius is not configured");
+    if (!slot_samples || !cell_starts || count != c->samples || cell_count != c->cells + 1)
+        return fail(c, BT_ERR_INVALID, "binning buffer sizes");
+    BT_CUDA(c, cudaMemcpyAsync(slot_samples, c->sorted_tag[c->cur].p, 4 * count, cudaMemcpyDeviceToHost, c->stream));
+    BT_CUDA(c, cudaMemcpyAsync(cell_starts, c->cell_start.p, 4 * cell_count, cudaMemcpyDeviceToHost, c->stream));
+    if (bt_status s = wait(c)) return s;
+    for (size_t i = 0; i < count; ++i) slot_samples[i] &= ~bt::kMovableBit;
+    return BT_OK;
+}
+
+bt_status bt_read_neighbors(bt_ctx* c, uint32_t* dst, size_t count) {
+    if (bt_status s = need_graph(c)) return s;
+    if (!c->has_grid) return fail(c, BT_ERR_NOT_CONFIGURED, "neighbor radius is not configured");
+    if (!c->opt.record_neighbors) return fail(c, BT_ERR_NOT_CONFIGURED, "neighbour counts are not recorded");
+    if (!dst || count != c->samples) return fail(c, BT_ERR_INVALID, "neighbor buffer size");
+    if (c->iterations == 0) {
+        std::memset(dst, 0, 4 * count);
+        return BT_OK;
+    }
+    if (bt_status s = ensure(c, c->records, 12ull * c->samples)) return s;
+    bt::launch_unsort_u32(c->neighbors.as<uint32_t>(), c->tmp_tag.as<uint32_t>(), c->samples,
+                          c->records.as<uint32_t>(), c->stream);
+    return copy_out(c, dst, c->records.p, 4 * count);
+}
+
+bt_status bt_distortion(bt_ctx* c, uint32_t size, double* distortion, double* rms_px) {
+    if (bt_status s = need_graph(c)) return s;
+    if (!c->opt.evaluate_distortion) return fail(c, BT_ERR_NOT_CONFIGURED, "distortion staging disabled");
+    if (!distortion || !rms_px || size == 0) return fail(c, BT_ERR_INVALID, "distortion viewport must be nonzero");
+    const float2* current = nullptr;
+    if (bt_status s = current_positions(c, &current)) return s;
+    if (bt_status s = ensure(c, c->integrals, 8ull * c->n_paths)) return s;
+    BT_CUDA(c, cudaMemsetAsync(c->status.p, 0, 4, c->stream));
+    bt::launch_edge_integrals(c->paths.as<bt::PathRec>(), c->n_paths, c->baseline.as<float2>(), current,
+                              c->integrals.as<double>(), c->status.as<uint32_t>(), c->stream);
+    std::vector<double> per_edge(c->n_paths);
+    std::vector<bt::PathRec> paths(c->n_paths);
+    BT_CUDA(c, cudaMemcpyAsync(per_edge.data(), c->integrals.p, 8ull * c->n_paths, cudaMemcpyDeviceToHost, c->stream));
+    BT_CUDA(c, cudaMemcpyAsync(paths.data(), c->paths.p, 12ull * c->n_paths, cudaMemcpyDeviceToHost, c->stream));
+    BT_CUDA(c, cudaMemcpyAsync(c->h_status, c->status.p, 4, cudaMemcpyDeviceToHost, c->stream));
+    if (bt_status s = wait(c)) return s;
+    if (c->h_status[0] & 4u) return fail(c, BT_ERR_INVALID, "nonfinite distortion curve or interval");
+    // Aggregate::add over edges in point-offset order (geometry.rs:64).
+    std::vector<uint32_t> order;
+    for (uint32_t e = 0; e < c->n_paths; ++e)
+        if (paths[e].count) order.push_back(e);
+    std::sort(order.begin(), order.end(),
+              [&](uint32_t a, uint32_t b) { return paths[a].point_offset < paths[b].point_offset; });
+    bt::KahanSum sum;
+    for (uint32_t e : order) {
+        bt::KahanSum trial = sum;
+        trial.add(per_edge[e]);
+        if (!std::isfinite(trial.value)) return fail(c, BT_ERR_INVALID, "nonfinite distortion aggregate");
+        sum = trial;
+    }
+    if (order.empty()) return fail(c, BT_ERR_INVALID, "distortion requires at least one edge");
+    // Aggregate::finish (distortion.rs:201-215)
+    const double rms = std::sqrt(sum.value / static_cast<double>(order.size()));
+    *distortion = rms / (2.0 * 1.4142135623730951);
+    *rms_px = rms * (static_cast<double>(size) / 2.0);
+    if (!std::isfinite(*distortion) || !std::isfinite(*rms_px))
+        return fail(c, BT_ERR_INVALID, "nonfinite distortion measurement");
+    return BT_OK;
+}
+
+bt_status bt_stage_times(bt_ctx* c, const char** names, float* ms, uint32_t capacity, uint32_t* count) {
+    if (!c || !count) return fail(c, BT_ERR_INVALID, "null argument");
+    if (bt_status s = wait(c)) return s;
+    // Sum per stage name over the last call, in first-seen order.
+    std::vector<const char*> seen;
+    std::vector<float> totals;
+    for (size_t i = 0; i < c->stage_used; ++i) {
+        const StageRec& r = c->stage_pool[i];
+        float t = 0.f;
+        cudaEventElapsedTime(&t, r.start, r.stop);
+        size_t k = 0;
+        while (k < seen.size() && std::strcmp(seen[k], r.name) != 0) ++k;
+        if (k == seen.size()) {
+            seen.push_back(r.name);
+            totals.push_back(0.f);
+        }
+        totals[k] += t;
+    }
+    *count = static_cast<uint32_t>(seen.size());
+    for (size_t k = 0; k < seen.size() && k < capacity; ++k) {
+        if (names) names[k] = seen[k];
+        if (ms) ms[k] = totals[k];
+    }
+    return BT_OK;
+}
+
+// ---- graph loader ----
+
+bt_status bt_graph_parse(const char* text, size_t len, bt_graph** out) {
+    if (!out || (!text && len)) return fail(nullptr, BT_ERR_INVALID, "null argument");
+    *out = nullptr;
+    auto* g = new bt_graph();
+    std::string err;
+    if (!bt::parse_trl(text ? text : "", len, &g->g, &err)) {
+        delete g;
+        return fail(nullptr, BT_ERR_INVALID, err);
+    }
+    *out = g;
+    return BT_OK;
+}
+
+bt_status bt_graph_load(const char* path, bt_graph** out) {
+    if (!out || !path) return fail(nullptr, BT_ERR_INVALID, "null argument");
+    *out = nullptr;
+    auto* g = new bt_graph();
+    std::string err;
+    if (!bt::load_trl(path, &g->g, &err)) {
+        delete g;
+        return fail(nullptr, BT_ERR_INVALID, err);
+    }
+    *out = g;
+    return BT_OK;
+}
+
+void bt_graph_free(bt_graph* g) { delete g; }
+uint32_t bt_graph_point_count(const bt_graph* g) { return g ? static_cast<uint32_t>(g->g.xy.size() / 2) : 0; }
+uint32_t bt_graph_start_count(const bt_graph* g) { return g ? static_cast<uint32_t>(g->g.starts.size()) : 0; }
+const float* bt_graph_points(const bt_graph* g) { return g ? g->g.xy.data() : nullptr; }
+const uint32_t* bt_graph_starts(const bt_graph* g) { return g ? g->g.starts.data() : nullptr; }
+
+bt_status bt_graph_normalization(const bt_graph* g, float out[5]) {
+    if (!g || !out) return fail(nullptr, BT_ERR_INVALID, "null argument");
+    std::string err;
+    if (!bt::normalization(g->g.min, g->g.max, out, &err)) return fail(nullptr, BT_ERR_INVALID, err);
+    return BT_OK;
+}
+
+// ---- geometry readers ----
+
+bt_status bt_layout_check(const uint32_t* paths, uint32_t n_paths, uint32_t samples) {
+    if (!paths && n_paths) return fail(nullptr, BT_ERR_INVALID, "null argument");
+    std::string err;
+    if (!bt::layout_check(paths, n_paths, samples, &err)) return fail(nullptr, BT_ERR_INVALID, err);
+    return BT_OK;
+}
+
+bt_status bt_decode_points(const uint32_t* paths, uint32_t n_paths, uint32_t samples, const void* records,
+                           size_t bytes, float* xy) {
+    if ((!paths && n_paths) || (!records && bytes) || !xy) return fail(nullptr, BT_ERR_INVALID, "null argument");
+    std::string err;
+    if (!bt::decode_points(paths, n_paths, samples, records, bytes, xy, &err)) return fail(nullptr, BT_ERR_INVALID, err);
+    return BT_OK;
+}
+
+bt_status bt_squared_integral(const float* original, size_t n_original, const float* current, size_t n_current,
+                              double* out) {
+    if (!original || !current || !out) return fail(nullptr, BT_ERR_INVALID, "null argument");
+    std::string err;
+    if (!bt::squared_integral_host(original, n_original, current, n_current, out, &err))
+        return fail(nullptr, BT_ERR_INVALID, err);
+    return BT_OK;
+}
+
+}  // extern "C"

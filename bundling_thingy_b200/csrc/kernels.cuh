@@ -1,0 +1,118 @@
+// kernels.cuh — launchers of the bundling kernels (one stream per context).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "common.cuh"
+
+namespace bt {
+
+// 12-byte path reservation (graph.wgsl Path; src/geometry.rs:8-12).
+struct PathRec {
+    uint32_t point_offset, segment_offset, count;
+};
+
+constexpr uint32_t kMovableBit = 0x80000000u;
+
+// ---- resampling (resample.cu) ----
+struct ResampleCountArgs {
+    const float2* cp;
+    const uint32_t* starts;
+    uint32_t paths;
+    Norm norm;
+    float sx, sy;            // resampling texel_scale
+    uint32_t capacity;
+    unsigned long long* packed;   // (count << 32) | 1 for paths with >= 2 samples, else 0
+    float4* edges;           // {first, last} control point per path
+    unsigned long long* totals;   // [0] samples, [1] drawn paths
+};
+void launch_resample_count(const ResampleCountArgs& a, cudaStream_t s);
+
+// Builds PathRec from the packed values and their exclusive scan.
+void launch_paths_from_scan(const unsigned long long* packed, const unsigned long long* scan, uint32_t paths,
+                            PathRec* out, cudaStream_t s);
+
+struct ResampleEmitArgs {
+    const float2* cp;
+    const uint32_t* starts;
+    const PathRec* paths;
+    uint32_t n_paths;
+    Norm norm;
+    float sx, sy;
+    Map map;
+    float2* xy;              // sample order
+    uint32_t* edge_ids;
+    uint32_t* segments;
+    uint32_t* counts;        // density splat (nullptr = off)
+    // binning for the first iteration (nullptr = no neighbour grid)
+    const Grid* grid_host;   // host copy (passed by value to the kernel)
+    uint32_t* tag;           // sample index | movable bit, sample order
+    uint32_t* cell;          // search cell of each sample
+    uint32_t* hist;          // search-cell populations
+    uint32_t* status;        // bit 1: count/emit mismatch
+};
+void launch_resample_emit(const ResampleEmitArgs& a, cudaStream_t s);
+
+// ---- density (density.cu) ----
+constexpr int kMaxTaps = 129;   // R <= 128
+struct Taps {
+    float w[kMaxTaps];
+    int R;
+};
+cudaError_t prepare_density_kernels();
+void launch_blur_horizontal(const uint32_t* counts, float* out, uint32_t w, uint32_t h, const Taps& taps,
+                            cudaStream_t s);
+void launch_blur_vertical(const float* in, float* out, uint32_t w, uint32_t h, const Taps& taps, uint32_t* peak,
+                          cudaStream_t s);
+void launch_normalize(const float* in, const uint32_t* peak, float* out, size_t n, cudaStream_t s);
+
+// ---- neighbour grid and mean (grid.cu) ----
+struct MeanArgs {
+    const float2* xy;        // slot order (sorted by search cell)
+    const int2* q;           // fixed-point positions, slot order
+    const uint32_t* tag;     // sample index | movable bit, slot order
+    const uint32_t* cell_start;
+    float2* out_xy;          // new positions, same slot order
+    uint32_t* out_tag;
+    uint32_t* out_cell;      // search cell of the new position
+    uint32_t* hist;          // populations of the next grid
+    uint32_t* counts;        // density splat (nullptr = off)
+    uint32_t* neighbors;     // |N(p)| per slot (nullptr = off)
+    uint32_t n;
+    Grid g;
+};
+void launch_neighbor_mean(const MeanArgs& a, cudaStream_t s);
+
+struct ScatterArgs {
+    const float2* xy;
+    const uint32_t* tag;
+    const uint32_t* cell;
+    const uint32_t* cell_start;
+    uint32_t* hist;          // counted down to zero
+    float2* out_xy;
+    int2* out_q;
+    uint32_t* out_tag;
+    uint32_t n;
+    uint32_t cells;          // search cells
+    uint32_t* status;        // bit 3 (value 8): inconsistent binning input
+};
+void launch_scatter(const ScatterArgs& a, cudaStream_t s);
+
+// Sample-order records {x, y, edge_id} from slot order.
+void launch_unsort_records(const float2* xy, const uint32_t* tag, const uint32_t* edge_ids, uint32_t n,
+                           uint32_t* records, cudaStream_t s);
+void launch_unsort_u32(const uint32_t* values, const uint32_t* tag, uint32_t n, uint32_t* out, cudaStream_t s);
+void launch_records_from_sample_order(const float2* xy, const uint32_t* edge_ids, uint32_t n, uint32_t* records,
+                                      cudaStream_t s);
+void launch_grid_cells(const float2* xy, const uint32_t* tag, uint32_t n, const Grid& g, uint32_t* out,
+                       cudaStream_t s);
+void launch_positions_from_slots(const float2* xy, const uint32_t* tag, uint32_t n, float2* out, cudaStream_t s);
+
+// ---- distortion (distortion.cu) ----
+// Per-edge squared_integral of original vs current (sample order); status bit
+// 2 (value 4) flags an invalid curve or interval.
+void launch_edge_integrals(const PathRec* paths, uint32_t n_paths, const float2* original, const float2* current,
+                           double* out, uint32_t* status, cudaStream_t s);
+
+}  // namespace bt

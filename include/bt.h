@@ -1,0 +1,201 @@
+/*
+ * bt.h — C ABI of the B200 (sm_100a) bundling library.
+ *
+ * Drop-in boundary for lpstankus/bundling_thingy's GPU bundling path: the
+ * `Gpu` type of the reference binary (src/gpu.rs), its graph loader
+ * (src/graph.rs) and the CPU readers of its GPU geometry (src/geometry.rs,
+ * src/distortion.rs). Plain pointers and sizes only; no CUDA or torch types.
+ *
+ * Conventions (mirroring the reference):
+ *  - Every call returns a bt_status; 0 is success. On failure a message is
+ *    available from bt_last_error(ctx) (ctx may be NULL for calls that fail
+ *    before a context exists). This replaces color_eyre::Result.
+ *  - A bt_ctx owns all device buffers of one graph (the reference's `Gpu`
+ *    owns its buffers and a new upload releases the previous graph,
+ *    src/gpu.rs:493-497). All calls on one context are serialised on that
+ *    context's CUDA stream; a context must not be used from two threads at
+ *    once. Different contexts are independent.
+ *  - Host buffers are owned by the caller; the library copies in and out.
+ *  - Blocking calls wait for the device with a deadline (60 s by default, as
+ *    `Gpu::wait`, src/gpu.rs:484-490) and return BT_ERR_TIMEOUT past it.
+ */
+#ifndef BT_H
+#define BT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BT_ABI_VERSION 1
+
+typedef int32_t bt_status;
+enum {
+    BT_OK = 0,
+    BT_ERR_CAPACITY = 1,       /* resampling exceeds sample capacity (resampling.wgsl overflow 1) */
+    BT_ERR_MISMATCH = 2,       /* count and emit passes disagree (resampling.wgsl overflow 2) */
+    BT_ERR_INVALID = 3,        /* invalid argument or input data */
+    BT_ERR_NO_GRAPH = 4,       /* no uploaded graph ("no uploaded graph", gpu.rs:440) */
+    BT_ERR_BUDGET = 5,         /* memory budget exhausted or device allocation failed */
+    BT_ERR_TIMEOUT = 6,        /* device wait deadline passed */
+    BT_ERR_CUDA = 7,           /* CUDA runtime error */
+    BT_ERR_NOT_CONFIGURED = 8  /* "neighbor radius is not configured" (gpu.rs:529-532) */
+};
+
+enum { BT_COLOR_BY_DENSITY = 0, BT_COLOR_BY_EDGE_ID = 1 };
+
+/* Options of Gpu::new (src/main.rs:34-90, src/gpu.rs:60-168). */
+typedef struct bt_options {
+    uint32_t width;                 /* map width in texels (headless reference: 1600, gpu.rs:21) */
+    uint32_t height;                /* map height in texels */
+    uint32_t neighbor_radius;       /* --neighbor-radius in texels; 0 = not configured */
+    uint32_t color_by;              /* --color-by; density enables the splat + blur passes */
+    uint64_t max_graph_memory_bytes;/* --max-graph-memory-mib * 2^20 (default 1024 MiB) */
+    uint32_t evaluate_distortion;   /* --evaluate-distortion: reserves staging bytes, keeps the baseline */
+    int32_t device;                 /* CUDA device ordinal */
+    /* Extensions beyond the reference (0 selects the reference behaviour): */
+    float sample_spacing;           /* resample spacing as a fraction of the canvas; 0 = one texel */
+    float blur_sigma;               /* Gaussian sigma in texels; 0 = the fixed sigma-6 table */
+    float blur_shrink;              /* sigma factor per density pass; 0 or 1 = none */
+    uint32_t fine_cells;            /* neighbour-search cells per grid cell side; 0 = automatic */
+    uint32_t use_graphs;            /* capture the iteration in a CUDA graph (1 = on, default) */
+    uint32_t timing;                /* record per-stage CUDA-event timings */
+    uint32_t record_neighbors;      /* keep |N(p)| of the last iteration for bt_read_neighbors */
+    uint32_t reserved[7];
+} bt_options;
+
+typedef struct bt_info {
+    uint32_t samples;         /* resampled points (Gpu::upload's return, gpu.rs:524) */
+    uint32_t paths;           /* edges in the uploaded graph */
+    uint32_t drawn_paths;     /* edges with at least two samples */
+    uint32_t segments;        /* samples - drawn_paths */
+    uint32_t capacity;        /* sample capacity from the budget (resampling.rs:363-370) */
+    uint32_t iterations;      /* neighbour-mean iterations since upload */
+    uint32_t grid_width;      /* neighbour grid cells (neighbor_mean.rs:26-32) */
+    uint32_t grid_height;
+    uint32_t fine_cells;      /* search cells per grid cell side */
+    uint32_t density_passes;  /* blur passes since upload */
+    uint64_t device_bytes;    /* device memory held by the context */
+    uint64_t reserved_bytes;  /* budget accounting of the reference (resampling.rs:394-395) */
+} bt_info;
+
+typedef struct bt_ctx bt_ctx;
+typedef struct bt_graph bt_graph;
+
+/* Library ABI version (BT_ABI_VERSION). */
+int32_t bt_abi_version(void);
+
+/* Fills the reference defaults: 1600x1600, density colouring, 1024 MiB. */
+void bt_options_init(bt_options* options);
+
+/* Gpu::new (src/gpu.rs:60-168). Validates the options like Resampler::new and
+ * GridBuffers::new (src/resampling.rs:72-96, src/neighbor_mean.rs:63-85). */
+bt_status bt_create(const bt_options* options, bt_ctx** out);
+
+/* Drop (releases the device buffers and the stream). NULL is ignored. */
+void bt_destroy(bt_ctx* ctx);
+
+/* Message of the last failure on ctx, or of the calling thread when ctx is NULL. */
+const char* bt_last_error(const bt_ctx* ctx);
+
+/* Gpu::upload (src/gpu.rs:493-525): resample the polylines into evenly spaced
+ * samples (resampling.wgsl count_paths/emit_paths), splat and blur the density
+ * (density.rs:150-166), and build the neighbour grid for the next iteration.
+ * xy holds 2*n_points floats; starts holds n_starts = edges + 1 offsets with
+ * starts[0] = 0 and starts[n_starts-1] = n_points (src/graph.rs:7-12). */
+bt_status bt_upload(bt_ctx* ctx, const float* xy, uint32_t n_points, const uint32_t* starts,
+                    uint32_t n_starts, uint32_t* out_samples);
+
+/* Upload of a parsed graph (Gpu::upload(&Graph)). */
+bt_status bt_upload_graph(bt_ctx* ctx, const bt_graph* graph, uint32_t* out_samples);
+
+/* Gpu::iterate (src/gpu.rs:527-553), n times: neighbour mean fused with the
+ * density splat, grid rebuild, blur and normalisation. Returns after the work
+ * has finished on the device. */
+bt_status bt_iterate(bt_ctx* ctx, uint32_t n);
+
+/* Enqueue n iterations without waiting (bt_synchronize waits). */
+bt_status bt_iterate_async(bt_ctx* ctx, uint32_t n);
+bt_status bt_synchronize(bt_ctx* ctx);
+
+/* bt_iterate, also returning the device milliseconds between CUDA events
+ * recorded on the context's stream before and after the n iterations (the
+ * reference logs per-pass gpu_ms, src/profiling.rs:127-133). */
+bt_status bt_iterate_timed(bt_ctx* ctx, uint32_t n, float* device_ms);
+
+bt_status bt_get_info(bt_ctx* ctx, bt_info* info);
+
+/* 12-byte little-endian {f32 x, f32 y, u32 edge_id} records, sample order
+ * (the point buffer read by distortion_snapshot, src/gpu.rs:469-482). */
+bt_status bt_read_points(bt_ctx* ctx, void* dst, size_t bytes);
+/* 12-byte {u32 point_offset, u32 segment_offset, u32 count} per edge
+ * (distortion_layout, src/gpu.rs:438-467). Skipped edges read as zeros. */
+bt_status bt_read_paths(bt_ctx* ctx, void* dst, size_t bytes);
+/* Segment start indices (resampling.wgsl segments buffer), samples - drawn_paths entries. */
+bt_status bt_read_segments(bt_ctx* ctx, uint32_t* dst, size_t count);
+/* Edge endpoints {x0, y0, x1, y1} per edge (resampling.wgsl edges buffer). */
+bt_status bt_read_edges(bt_ctx* ctx, float* dst, size_t count);
+/* Normalised density, width*height f32 in [0,1] (normalization.wgsl; the
+ * reference stores it in the R channel of an RGBA16F texture). */
+bt_status bt_read_density(bt_ctx* ctx, float* dst, size_t count);
+/* Blurred density before normalisation and its maximum (blur.wgsl outputs). */
+bt_status bt_read_density_raw(bt_ctx* ctx, float* dst, size_t count, float* peak);
+/* Splat counts of the last density pass, width*height u32. */
+bt_status bt_read_counts(bt_ctx* ctx, uint32_t* dst, size_t count);
+/* Neighbour-grid cell ids (spatial_grid.wgsl:67-70) of the current samples,
+ * sample order. Requires a configured radius. */
+bt_status bt_read_cells(bt_ctx* ctx, uint32_t* dst, size_t count);
+/* The grid binning that the next iteration will search: samples listed by
+ * search cell (slot order, `count` = samples) and the start slot of each
+ * search cell (cell_count = fine grid cells + 1). */
+bt_status bt_read_binning(bt_ctx* ctx, uint32_t* slot_samples, size_t count, uint32_t* cell_starts,
+                          size_t cell_count);
+/* Neighbour count |N(p)| of every sample in the last iteration (0 for
+ * endpoints), sample order. */
+bt_status bt_read_neighbors(bt_ctx* ctx, uint32_t* dst, size_t count);
+
+/* Distortion of the current geometry against the geometry at upload
+ * (src/main.rs:159-180, src/distortion.rs:172-216); requires
+ * evaluate_distortion. size is the canvas size in pixels (gpu::SIZE). */
+bt_status bt_distortion(bt_ctx* ctx, uint32_t size, double* distortion, double* rms_displacement_pixels);
+
+/* Per-stage device milliseconds of the last upload/iteration, as the
+ * reference's GpuTimings (src/profiling.rs:35-136). names/ms hold `capacity`
+ * entries; returns the number of stages in *count. */
+bt_status bt_stage_times(bt_ctx* ctx, const char** names, float* ms, uint32_t capacity, uint32_t* count);
+
+/* ---- Graph loader (src/graph.rs) ---- */
+
+/* Graph::parse (src/graph.rs:35-77). */
+bt_status bt_graph_parse(const char* text, size_t len, bt_graph** out);
+/* Graph::load (src/graph.rs:22-33). */
+bt_status bt_graph_load(const char* path, bt_graph** out);
+void bt_graph_free(bt_graph* graph);
+uint32_t bt_graph_point_count(const bt_graph* graph);
+uint32_t bt_graph_start_count(const bt_graph* graph);
+const float* bt_graph_points(const bt_graph* graph);      /* Graph::points, 2 floats per point */
+const uint32_t* bt_graph_starts(const bt_graph* graph);   /* Graph::starts */
+/* Graph::normalization (src/graph.rs:79-91): {min_x, min_y, scale, tx, ty}. */
+bt_status bt_graph_normalization(const bt_graph* graph, float out[5]);
+
+/* ---- CPU readers of GPU geometry (src/geometry.rs, src/distortion.rs) ---- */
+
+/* Layout::new (src/geometry.rs:28-73): checks that path reservations tile
+ * [0, samples) and segments tile [0, samples - edges). paths holds 3 u32 per
+ * edge. Returns BT_ERR_INVALID with the reference's message otherwise. */
+bt_status bt_layout_check(const uint32_t* paths, uint32_t n_paths, uint32_t samples);
+/* Decoder::push/finish (src/geometry.rs:131-187): decodes 12-byte records to
+ * 2 floats per sample, checking edge ids and finiteness. */
+bt_status bt_decode_points(const uint32_t* paths, uint32_t n_paths, uint32_t samples, const void* records,
+                           size_t bytes, float* xy);
+/* squared_integral (src/distortion.rs:137-168) of two f32 curves. */
+bt_status bt_squared_integral(const float* original, size_t n_original, const float* current,
+                              size_t n_current, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BT_H */
