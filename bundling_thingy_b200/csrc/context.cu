@@ -239,8 +239,8 @@ bt_status enqueue_density(bt_ctx* c, uint32_t pass) {
 // Scan of the search-cell populations and the scatter into slot order `dst`.
 void enqueue_binning(bt_ctx* c, int dst) {
     stage_begin(c, "graph.grid_scan");
-    bt::exclusive_scan<uint32_t>(c->hist.as<uint32_t>(), c->cell_start.as<uint32_t>(), c->cells,
-                                 c->scan32.as<uint32_t>(), c->stream);
+    bt::exclusive_scan<uint32_t, uint32_t>(c->hist.as<uint32_t>(), c->cell_start.as<uint32_t>(), c->cells,
+                                           c->scan32.as<uint32_t>(), c->stream);
     stage_end(c);
     stage_begin(c, "graph.grid_scatter");
     bt::ScatterArgs s{};
@@ -524,8 +524,9 @@ bt_status bt_upload(bt_ctx* c, const float* xy, uint32_t n_points, const uint32_
     const uint32_t segs = static_cast<uint32_t>(total - drawn);
 
     stage_begin(c, "graph.emit");
-    bt::exclusive_scan<unsigned long long>(c->packed.as<unsigned long long>(), c->offsets.as<unsigned long long>(), E,
-                                           c->scan64.as<unsigned long long>(), c->stream);
+    bt::exclusive_scan<unsigned long long, unsigned long long>(c->packed.as<unsigned long long>(),
+                                                               c->offsets.as<unsigned long long>(), E,
+                                                               c->scan64.as<unsigned long long>(), c->stream);
     bt::launch_paths_from_scan(c->packed.as<unsigned long long>(), c->offsets.as<unsigned long long>(), E,
                                c->paths.as<bt::PathRec>(), c->stream);
     if (bt_status s = ensure(c, c->edge_ids, 4ull * N)) return s;
