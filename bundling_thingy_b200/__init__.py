@@ -100,6 +100,7 @@ SIGNATURES = {
     "bt_read_neighbors": ([_vp, _u32p, ctypes.c_size_t], ctypes.c_int32),
     "bt_distortion": ([_vp, ctypes.c_uint32, _f64p, _f64p], ctypes.c_int32),
     "bt_stage_times": ([_vp, ctypes.POINTER(ctypes.c_char_p), _f32p, ctypes.c_uint32, _u32p], ctypes.c_int32),
+    "bt_density_noalloc": ([_vp, _vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_float, _vp], ctypes.c_int32),
     "bt_graph_parse": ([ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(_vp)], ctypes.c_int32),
     "bt_graph_load": ([ctypes.c_char_p, ctypes.POINTER(_vp)], ctypes.c_int32),
     "bt_graph_free": ([_vp], None),

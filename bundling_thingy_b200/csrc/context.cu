@@ -314,6 +314,12 @@ bt_status validate_options(const bt_options* o, bt_ctx* c) {
 
 }  // namespace
 
+namespace bt {
+// Shared with the allocation-free density entry point (density_noalloc.cu).
+bool make_blur_taps(double sigma, Taps* taps) { return blur_taps(sigma, taps); }
+void set_thread_error(const char* message) { g_thread_error = message; }
+}  // namespace bt
+
 extern "C" {
 
 int32_t bt_abi_version(void) { return BT_ABI_VERSION; }

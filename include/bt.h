@@ -166,6 +166,33 @@ bt_status bt_distortion(bt_ctx* ctx, uint32_t size, double* distortion, double* 
  * entries; returns the number of stages in *count. */
 bt_status bt_stage_times(bt_ctx* ctx, const char** names, float* ms, uint32_t capacity, uint32_t* count);
 
+/* ---- Density blur without allocation ---- */
+
+/* Largest width*height accepted by bt_density_noalloc: its static device
+ * scratch holds one f32 image of this many texels (4 MiB) plus a 256-byte
+ * head, on every GPU that loads the library, until the process exits. */
+#define BT_NOALLOC_MAX_TEXELS (1024u * 1024u)
+
+/* No counterpart in the reference. The density blur and normalisation
+ * (the same kernels and results as the density passes of bt_upload and
+ * bt_iterate) for callers that may not allocate device memory: a plugin or
+ * renderer whose host application owns every device allocation, or a frame
+ * loop that cannot take cudaMalloc's implicit device synchronisation or an
+ * allocation failure mid-frame. The caller passes device pointers to
+ * width*height u32 splat counts and to the width*height f32 output, and a
+ * cudaStream_t as `stream` (NULL = the default stream); the call is
+ * asynchronous on that stream. It calls no cudaMalloc or cudaFree: its one
+ * intermediate image lives in a file-scope static device array of
+ * BT_NOALLOC_MAX_TEXELS texels, and larger maps are rejected with
+ * BT_ERR_INVALID. The first call on a device performs a one-time set-up on
+ * the current device (the array's device address and the kernels'
+ * shared-memory attribute); make that first call before any stream capture.
+ * Every call shares the one array per device, so calls whose work overlaps on
+ * the GPU race: serialise them (one stream, or events between streams).
+ * blur_sigma as bt_options.blur_sigma (0 = the fixed sigma-6 table). */
+bt_status bt_density_noalloc(const uint32_t* counts, float* density, uint32_t width, uint32_t height,
+                             float blur_sigma, void* stream);
+
 /* ---- Graph loader (src/graph.rs) ---- */
 
 /* Graph::parse (src/graph.rs:35-77). */
