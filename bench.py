@@ -296,26 +296,30 @@ def run_ours(args, ranks: Ranks):
 
     # End to end through the public API with host buffers: upload the control
     # points, 30 iterations, read back the 12-byte records and the density.
-    opts_e2e = bt.Options(width=w.width, height=w.height, neighbor_radius=w.radius, sample_spacing=w.spacing,
-                          blur_sigma=w.sigma, device=device)
-    e2e_gpu = bt.Gpu(opts_e2e)
-    records = np.empty(12 * n, np.uint8)
-    job_times = []
-    for j in range(args.e2e_jobs + 1):
-        ranks.barrier()
-        t0 = time.perf_counter()
-        m = e2e_gpu.upload((w.xy, w.starts))
-        e2e_gpu.iterate(ITERATIONS_PER_JOB)
-        bt.library().bt_read_points(e2e_gpu._h, records.ctypes.data, records.size)
-        dens = e2e_gpu.read_density()
-        t = time.perf_counter() - t0
-        if j > 0:  # the first job warms host paths
-            job_times.append(t)
-    e2e_gpu.close()
-    job = ranks.max(statistics.median(job_times))
-    e2e_value = ranks.sum(float(n) * ITERATIONS_PER_JOB) / job
-    h2d = w.xy.nbytes + w.starts.nbytes
-    d2h = records.nbytes + dens.nbytes
+    # (--e2e-jobs 0 skips it, for short profiling runs.)
+    e2e_value = job = None
+    h2d = d2h = 0
+    if args.e2e_jobs > 0:
+        opts_e2e = bt.Options(width=w.width, height=w.height, neighbor_radius=w.radius, sample_spacing=w.spacing,
+                              blur_sigma=w.sigma, device=device)
+        e2e_gpu = bt.Gpu(opts_e2e)
+        records = np.empty(12 * n, np.uint8)
+        job_times = []
+        for j in range(args.e2e_jobs + 1):
+            ranks.barrier()
+            t0 = time.perf_counter()
+            e2e_gpu.upload((w.xy, w.starts))
+            e2e_gpu.iterate(ITERATIONS_PER_JOB)
+            bt.library().bt_read_points(e2e_gpu._h, records.ctypes.data, records.size)
+            dens = e2e_gpu.read_density()
+            t = time.perf_counter() - t0
+            if j > 0:  # the first job warms host paths
+                job_times.append(t)
+        e2e_gpu.close()
+        job = ranks.max(statistics.median(job_times))
+        e2e_value = ranks.sum(float(n) * ITERATIONS_PER_JOB) / job
+        h2d = w.xy.nbytes + w.starts.nbytes
+        d2h = records.nbytes + dens.nbytes
 
     cpu = None
     if ranks.rank == 0 and ranks.world == 1 and not args.no_cpu_baseline:

@@ -61,7 +61,7 @@ class _Options(ctypes.Structure):
         ("evaluate_distortion", ctypes.c_uint32), ("device", ctypes.c_int32),
         ("sample_spacing", ctypes.c_float), ("blur_sigma", ctypes.c_float), ("blur_shrink", ctypes.c_float),
         ("fine_cells", ctypes.c_uint32), ("use_graphs", ctypes.c_uint32), ("timing", ctypes.c_uint32),
-        ("record_neighbors", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 7),
+        ("record_neighbors", ctypes.c_uint32), ("search_mode", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 6),
     ]
 
 
@@ -174,6 +174,7 @@ class Options:
     use_graphs: bool = True
     timing: bool = False
     record_neighbors: bool = False
+    search_mode: int = 0     # 0: interior cells by prefix sums; 1: test every candidate (same results)
 
     def _struct(self) -> _Options:
         o = _Options()
@@ -191,6 +192,7 @@ class Options:
         o.use_graphs = int(bool(self.use_graphs))
         o.timing = int(bool(self.timing))
         o.record_neighbors = int(bool(self.record_neighbors))
+        o.search_mode = int(self.search_mode)
         return o
 
     def resample_scale(self) -> tuple[float, float]:

@@ -65,7 +65,7 @@ struct bt_ctx {
 
     DevBuf cp, starts, packed, offsets, scan64, edges, paths, totals, status;
     DevBuf edge_ids, segments, tmp_xy, tmp_tag, tmp_cell, neighbors, baseline, current;
-    DevBuf sorted_xy[2], sorted_q[2], sorted_tag[2];
+    DevBuf sorted_rec[2], sorted_tag[2], prefix, prefix_scratch;
     DevBuf hist, cell_start, scan32;
     DevBuf counts, himg, vimg, norm, peak;
     DevBuf records, integrals;
@@ -249,14 +249,19 @@ void enqueue_binning(bt_ctx* c, int dst) {
     s.cell = c->tmp_cell.as<uint32_t>();
     s.cell_start = c->cell_start.as<uint32_t>();
     s.hist = c->hist.as<uint32_t>();
-    s.out_xy = c->sorted_xy[dst].as<float2>();
-    s.out_q = c->sorted_q[dst].as<int2>();
+    s.out_rec = c->sorted_rec[dst].as<uint4>();
     s.out_tag = c->sorted_tag[dst].as<uint32_t>();
     s.n = c->samples;
     s.cells = static_cast<uint32_t>(c->cells);
     s.status = c->status.as<uint32_t>();
     bt::launch_scatter(s, c->stream);
     stage_end(c);
+    if (c->opt.search_mode == bt::kSearchInterior) {
+        stage_begin(c, "graph.position_prefix");
+        bt::launch_position_prefix(c->sorted_rec[dst].as<uint4>(), c->samples, c->prefix.as<bt::LL2>(),
+                                   c->prefix_scratch.as<bt::LL2>(), c->stream);
+        stage_end(c);
+    }
 }
 
 // One Gpu::iterate (gpu.rs:527-553) starting from slot order `src`.
@@ -267,10 +272,11 @@ bt_status enqueue_iteration(bt_ctx* c, int src, uint32_t pass) {
     }
     stage_begin(c, "graph.neighbor_mean");
     bt::MeanArgs m{};
-    m.xy = c->sorted_xy[src].as<float2>();
-    m.q = c->sorted_q[src].as<int2>();
+    m.rec = c->sorted_rec[src].as<uint4>();
     m.tag = c->sorted_tag[src].as<uint32_t>();
     m.cell_start = c->cell_start.as<uint32_t>();
+    m.prefix = c->prefix.as<bt::LL2>();
+    m.mode = static_cast<int>(c->opt.search_mode);
     m.out_xy = c->tmp_xy.as<float2>();
     m.out_tag = c->tmp_tag.as<uint32_t>();
     m.out_cell = c->tmp_cell.as<uint32_t>();
@@ -302,6 +308,7 @@ bt_status validate_options(const bt_options* o, bt_ctx* c) {
     if (o->sample_spacing > 0.0f && !std::isfinite(0.5 / static_cast<double>(o->sample_spacing)))
         return fail(c, BT_ERR_INVALID, "invalid sample spacing");
     if (o->neighbor_radius > 0 && o->fine_cells > 4096) return fail(c, BT_ERR_INVALID, "fine_cells too large");
+    if (o->search_mode > 1) return fail(c, BT_ERR_INVALID, "unknown search_mode");
     const uint64_t grid = o->neighbor_radius ? reference_grid_bytes(o->width, o->height, o->neighbor_radius) : 0;
     const uint64_t staging = o->evaluate_distortion ? kDistortionStagingBytes : 0;
     // resampling.rs:85-89
@@ -424,8 +431,8 @@ void bt_destroy(bt_ctx* c) {
     drop_graphs(c);
     DevBuf* bufs[] = {&c->cp, &c->starts, &c->packed, &c->offsets, &c->scan64, &c->edges, &c->paths, &c->totals,
                       &c->status, &c->edge_ids, &c->segments, &c->tmp_xy, &c->tmp_tag, &c->tmp_cell,
-                      &c->neighbors, &c->baseline, &c->current, &c->sorted_xy[0], &c->sorted_xy[1],
-                      &c->sorted_q[0], &c->sorted_q[1], &c->sorted_tag[0], &c->sorted_tag[1], &c->hist,
+                      &c->neighbors, &c->baseline, &c->current, &c->sorted_rec[0], &c->sorted_rec[1],
+                      &c->prefix, &c->prefix_scratch, &c->sorted_tag[0], &c->sorted_tag[1], &c->hist,
                       &c->cell_start, &c->scan32, &c->counts, &c->himg, &c->vimg, &c->norm, &c->peak,
                       &c->records, &c->integrals};
     for (DevBuf* b : bufs) release(*b);
@@ -542,9 +549,13 @@ bt_status bt_upload(bt_ctx* c, const float* xy, uint32_t n_points, const uint32_
     if (bt_status s = ensure(c, c->tmp_cell, 4ull * N)) return s;
     if (c->has_grid) {
         for (int b = 0; b < 2; ++b) {
-            if (bt_status s = ensure(c, c->sorted_xy[b], 8ull * N)) return s;
-            if (bt_status s = ensure(c, c->sorted_q[b], 8ull * N)) return s;
+            if (bt_status s = ensure(c, c->sorted_rec[b], 16ull * N)) return s;
             if (bt_status s = ensure(c, c->sorted_tag[b], 4ull * N)) return s;
+        }
+        if (c->opt.search_mode == bt::kSearchInterior) {
+            if (bt_status s = ensure(c, c->prefix, sizeof(bt::LL2) * (N + 1ull))) return s;
+            if (bt_status s = ensure(c, c->prefix_scratch, sizeof(bt::LL2) * bt::position_prefix_scratch(N)))
+                return s;
         }
         if (c->opt.record_neighbors)
             if (bt_status s = ensure(c, c->neighbors, 4ull * N)) return s;
@@ -723,7 +734,7 @@ bt_status current_positions(bt_ctx* c, const float2** out) {
         return BT_OK;
     }
     if (bt_status s = ensure(c, c->current, 8ull * c->samples)) return s;
-    bt::launch_positions_from_slots(c->sorted_xy[c->cur].as<float2>(), c->sorted_tag[c->cur].as<uint32_t>(),
+    bt::launch_positions_from_slots(c->sorted_rec[c->cur].as<uint4>(), c->sorted_tag[c->cur].as<uint32_t>(),
                                     c->samples, c->current.as<float2>(), c->stream);
     *out = c->current.as<float2>();
     return BT_OK;
@@ -736,7 +747,7 @@ bt_status bt_read_points(bt_ctx* c, void* dst, size_t bytes) {
     if (!dst || bytes != 12ull * c->samples) return fail(c, BT_ERR_INVALID, "point buffer must hold 12 bytes per sample");
     if (bt_status s = ensure(c, c->records, 12ull * c->samples)) return s;
     if (c->has_grid) {
-        bt::launch_unsort_records(c->sorted_xy[c->cur].as<float2>(), c->sorted_tag[c->cur].as<uint32_t>(),
+        bt::launch_unsort_records(c->sorted_rec[c->cur].as<uint4>(), c->sorted_tag[c->cur].as<uint32_t>(),
                                   c->edge_ids.as<uint32_t>(), c->samples, c->records.as<uint32_t>(), c->stream);
     } else {
         bt::launch_records_from_sample_order(c->tmp_xy.as<float2>(), c->edge_ids.as<uint32_t>(), c->samples,
@@ -795,7 +806,7 @@ bt_status bt_read_cells(bt_ctx* c, uint32_t* dst, size_t count) {
     if (!c->has_grid) return fail(c, BT_ERR_NOT_CONFIGURED, "neighbor radius is not configured");
     if (!dst || count != c->samples) return fail(c, BT_ERR_INVALID, "cell buffer must hold one id per sample");
     if (bt_status s = ensure(c, c->records, 12ull * c->samples)) return s;
-    bt::launch_grid_cells(c->sorted_xy[c->cur].as<float2>(), c->sorted_tag[c->cur].as<uint32_t>(), c->samples,
+    bt::launch_grid_cells(c->sorted_rec[c->cur].as<uint4>(), c->sorted_tag[c->cur].as<uint32_t>(), c->samples,
                           c->grid, c->records.as<uint32_t>(), c->stream);
     return copy_out(c, dst, c->records.p, 4 * count);
 }

@@ -7,76 +7,138 @@
 // Semantics (identical to the oracle): N(p) = every sample q whose grid cell
 // lies in p's reach box (grid_cell(texel(p) -/+ reach)) and that passes the
 // reference's f32 test dot((q-p)*ts, (q-p)*ts) <= r*r. The displacement is
-// accumulated exactly in 2^-30 fixed point (int64), so the result does not
-// depend on the order of N(p) — which the reference leaves to atomics — and
-// p' = p + f32(f64(sum) / (f64(|N|) * 2^30)).
+// accumulated exactly in 2^-30 fixed point (64-bit integers), so the result
+// does not depend on the order of N(p) — which the reference leaves to
+// atomics — nor on how N(p) is enumerated:
+//   p' = p + f32(f64(sum_q Q(q) - |N| Q(p)) / (f64(|N|) * 2^30)).
 //
-// B200 layout: samples live in slot order, sorted by search cell (each grid
-// cell side split into k search cells, search cells row-major over the whole
-// map). A search row of cells [a, b] is then one contiguous slot range, so a
-// thread walks, row by row, only the search cells that can meet its circle
-// (conservative chord bounds), testing every sample there exactly. The kernel
-// writes the new position in the same slot order (coalesced), its next search
-// cell and population count (fusing count_cells of the next iteration), and
-// its density splat. The scatter then moves the samples into the next slot
-// order, counting the populations back down to zero for reuse.
+// B200 layout: samples live in slot order as 16-byte records
+// {x, y, Q(x) + 2^30, Q(y) + 2^30}, sorted by search cell (each grid cell side
+// split into k search cells, search cells row-major over the whole map), so a
+// row of search cells [a, b] is one contiguous slot range. An exclusive prefix
+// sum of the biased fixed-point positions over slots turns any such range into
+// one subtraction. Per search row, a thread takes the cells that lie entirely
+// inside its circle (by conservative bounds, with a margin far above every
+// f32 rounding involved) from the prefix sums — the role of the reference's
+// fully-contained cell summaries (neighbor_mean.wgsl:40-59) — and tests only
+// the samples of the boundary cells, exactly. The kernel writes the new
+// position in the same slot order (coalesced), its next search cell and the
+// population count (fusing count_cells of the next iteration), and its density
+// splat. The scatter then moves the samples into the next slot order,
+// counting the populations back down to zero for reuse.
 #include "kernels.cuh"
 
 namespace bt {
 namespace {
 
 __device__ __forceinline__ int floor_div(float t, float s) { return static_cast<int>(floorf(t / s)); }
+__device__ __forceinline__ int ceil_div(float t, float s) { return static_cast<int>(ceilf(t / s)); }
+
+// Approximate square root (one MUFU op); callers widen its result by a
+// relative 1e-6 plus the margin, far above its error.
+__device__ __forceinline__ float sqrt_approx(float x) {
+    float r;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+struct Acc {
+    unsigned long long sx, sy;
+    uint32_t count;
+};
+
+// Exact test of every sample in slots [b, e) (neighbor_mean.wgsl:193-198).
+__device__ __forceinline__ void scan_range(const uint4* __restrict__ rec, uint32_t b, uint32_t e, float2 neg_p,
+                                           float2 ts, float r2, Acc& acc) {
+#pragma unroll 4
+    for (uint32_t j = b; j < e; ++j) {
+        const uint4 q = __ldg(rec + j);
+        const float2 d = __fadd2_rn(make_float2(__uint_as_float(q.x), __uint_as_float(q.y)), neg_p);
+        const float2 t = __fmul2_rn(d, ts);
+        const float2 t2 = __fmul2_rn(t, t);
+        const float d2 = t2.x + t2.y;
+        if (d2 <= r2) {
+            acc.sx += q.z;
+            acc.sy += q.w;
+            acc.count += 1u;
+        }
+    }
+}
 
 __global__ void __launch_bounds__(256) neighbor_mean_kernel(MeanArgs a) {
     const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
     if (slot >= a.n) return;
     const Grid& g = a.g;
-    const float2 p = a.xy[slot];
+    const uint4 me = a.rec[slot];
+    const float2 p = make_float2(__uint_as_float(me.x), __uint_as_float(me.y));
     const uint32_t tag = a.tag[slot];
     float2 np = p;
     uint32_t count = 0;
     if (tag & kMovableBit) {
         const float tx = texel_of(p.x, g.map.wm1), ty = texel_of(p.y, g.map.hm1);
-        // Reach box in grid cells (neighbor_mean.wgsl:180-185).
+        // Reach box in grid cells (neighbor_mean.wgsl:180-185), in search cells.
         const uint32_t cx0 = grid_of(tx - g.reachx, g.rf, g.gw), cx1 = grid_of(tx + g.reachx, g.rf, g.gw);
         const uint32_t cy0 = grid_of(ty - g.reachy, g.rf, g.gh), cy1 = grid_of(ty + g.reachy, g.rf, g.gh);
         const int fx_min = static_cast<int>(cx0 * g.k), fx_max = static_cast<int>(cx1 * g.k + g.k - 1u);
         const int fy_min = static_cast<int>(cy0 * g.k), fy_max = static_cast<int>(cy1 * g.k + g.k - 1u);
-        // Conservative circle: radius r + margin around the texel position.
+        // Candidate circle r + m; certain circle r - m (texels).
         const float R = g.rf + g.margin;
+        const float Rin = g.rf - g.margin;
         const int fy_lo = max(fy_min, floor_div(ty - R, g.s));
         const int fy_hi = min(fy_max, floor_div(ty + R, g.s));
-        const int2 qp = a.q[slot];
-        long long sx = 0, sy = 0;
+        const bool interior = a.mode == kSearchInterior;
+        const int fw = static_cast<int>(g.fw), fh = static_cast<int>(g.fh);
+        const float2 neg_p = make_float2(-p.x, -p.y);
+        const float2 ts = make_float2(g.tsx, g.tsy);
+        Acc acc{0ull, 0ull, 0u};
         for (int fy = fy_lo; fy <= fy_hi; ++fy) {
             const float ylo = static_cast<float>(fy) * g.s;
             const float yhi = ylo + g.s;
-            float dy = fmaxf(fmaxf(ylo - ty, ty - yhi), 0.0f) - g.margin;
-            dy = fmaxf(dy, 0.0f);
-            if (dy > R) continue;
-            const float half = sqrtf(fmaxf(R * R - dy * dy, 0.0f)) + g.margin;
-            const int fx_lo = max(fx_min, floor_div(tx - half, g.s));
-            const int fx_hi = min(fx_max, floor_div(tx + half, g.s));
-            if (fx_lo > fx_hi) continue;
+            const float near = fmaxf(fmaxf(ylo - ty, ty - yhi), 0.0f);
+            const float dn = fmaxf(near - g.margin, 0.0f);
+            if (dn > R) continue;
+            // f32 rounding of R^2 - dn^2 is below 5e-7 R^2; widen by that.
+            const float hout = sqrt_approx(fmaxf(R * R - dn * dn + 5e-7f * R * R, 0.0f)) * 1.000001f + g.margin;
+            const int bx0 = max(fx_min, floor_div(tx - hout, g.s));
+            const int bx1 = min(fx_max, floor_div(tx + hout, g.s));
+            if (bx0 > bx1) continue;
             const uint32_t row = static_cast<uint32_t>(fy) * g.fw;
-            const uint32_t b = a.cell_start[row + fx_lo];
-            const uint32_t e = a.cell_start[row + fx_hi + 1];
-            for (uint32_t j = b; j < e; ++j) {
-                const float2 qq = a.xy[j];
-                const float dx = qq.x - p.x, ddy = qq.y - p.y;
-                const float ex = dx * g.tsx, ey = ddy * g.tsy;
-                const float d2 = ex * ex + ey * ey;
-                if (d2 <= g.r2) {
-                    const int2 qj = a.q[j];
-                    sx += static_cast<long long>(qj.x) - static_cast<long long>(qp.x);
-                    sy += static_cast<long long>(qj.y) - static_cast<long long>(qp.y);
-                    ++count;
+            const uint32_t s0 = a.cell_start[row + bx0];
+            const uint32_t s3 = a.cell_start[row + bx1 + 1];
+            int ix0 = 1, ix1 = 0;
+            if (interior && fy > 0 && fy < fh - 1) {
+                // Cells of this row whose every sample passes the f32 test:
+                // the farthest point of the row band, widened by the margin.
+                const float far = fmaxf(fabsf(ylo - ty), fabsf(yhi - ty)) + g.margin;
+                if (far < Rin) {
+                    const float h2 = Rin * Rin - far * far - 5e-7f * Rin * Rin;
+                    const float hin = sqrt_approx(fmaxf(h2, 0.0f)) * 0.999999f - g.margin;
+                    if (hin > 0.0f) {
+                        ix0 = max(ceil_div(tx - hin, g.s), max(bx0, 1));
+                        ix1 = min(floor_div(tx + hin, g.s) - 1, min(bx1, fw - 2));
+                    }
                 }
             }
+            if (ix0 <= ix1) {
+                const uint32_t s1 = a.cell_start[row + ix0];
+                const uint32_t s2 = a.cell_start[row + ix1 + 1];
+                const LL2 lo = a.prefix[s1], hi = a.prefix[s2];
+                acc.sx += static_cast<unsigned long long>(hi.x - lo.x);
+                acc.sy += static_cast<unsigned long long>(hi.y - lo.y);
+                acc.count += s2 - s1;
+                scan_range(a.rec, s0, s1, neg_p, ts, g.r2, acc);
+                scan_range(a.rec, s2, s3, neg_p, ts, g.r2, acc);
+            } else {
+                scan_range(a.rec, s0, s3, neg_p, ts, g.r2, acc);
+            }
         }
+        count = acc.count;
+        // Biased sums: sum (Q(q) + B) - n (Q(p) + B) = sum Q(q) - n Q(p).
+        const long long dx = static_cast<long long>(acc.sx - static_cast<unsigned long long>(count) * me.z);
+        const long long dy = static_cast<long long>(acc.sy - static_cast<unsigned long long>(count) * me.w);
         const double den = static_cast<double>(count) * 1073741824.0;
-        np.x = p.x + static_cast<float>(static_cast<double>(sx) / den);
-        np.y = p.y + static_cast<float>(static_cast<double>(sy) / den);
+        np.x = p.x + static_cast<float>(static_cast<double>(dx) / den);
+        np.y = p.y + static_cast<float>(static_cast<double>(dy) / den);
     }
     a.out_xy[slot] = np;
     a.out_tag[slot] = tag;
@@ -110,19 +172,20 @@ __global__ void __launch_bounds__(256) scatter_kernel(ScatterArgs a) {
         return;
     }
     const float2 p = a.xy[i];
-    a.out_xy[slot] = p;
-    a.out_q[slot] = make_int2(__float2int_rn(p.x * kFixedScale), __float2int_rn(p.y * kFixedScale));
+    const uint32_t qx = static_cast<uint32_t>(__float2int_rn(p.x * kFixedScale)) + kFixedBias;
+    const uint32_t qy = static_cast<uint32_t>(__float2int_rn(p.y * kFixedScale)) + kFixedBias;
+    a.out_rec[slot] = make_uint4(__float_as_uint(p.x), __float_as_uint(p.y), qx, qy);
     a.out_tag[slot] = a.tag[i];
 }
 
-__global__ void unsort_records_kernel(const float2* xy, const uint32_t* tag, const uint32_t* edge_ids, uint32_t n,
+__global__ void unsort_records_kernel(const uint4* rec, const uint32_t* tag, const uint32_t* edge_ids, uint32_t n,
                                       uint32_t* records) {
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n) return;
     const uint32_t i = tag[s] & ~kMovableBit;
-    const float2 p = xy[s];
-    records[3 * static_cast<size_t>(i)] = __float_as_uint(p.x);
-    records[3 * static_cast<size_t>(i) + 1] = __float_as_uint(p.y);
+    const uint4 r = rec[s];
+    records[3 * static_cast<size_t>(i)] = r.x;
+    records[3 * static_cast<size_t>(i) + 1] = r.y;
     records[3 * static_cast<size_t>(i) + 2] = edge_ids[i];
 }
 
@@ -142,20 +205,20 @@ __global__ void records_kernel(const float2* xy, const uint32_t* edge_ids, uint3
 }
 
 // cell_index (spatial_grid.wgsl:67-70) of each sample, sample order.
-__global__ void grid_cells_kernel(const float2* xy, const uint32_t* tag, uint32_t n, Grid g, uint32_t* out) {
+__global__ void grid_cells_kernel(const uint4* rec, const uint32_t* tag, uint32_t n, Grid g, uint32_t* out) {
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n) return;
-    const float2 p = xy[s];
-    const uint32_t cx = grid_of(texel_of(p.x, g.map.wm1), g.rf, g.gw);
-    const uint32_t cy = grid_of(texel_of(p.y, g.map.hm1), g.rf, g.gh);
-    const uint32_t i = tag ? (tag[s] & ~kMovableBit) : s;
-    out[i] = cy * g.gw + cx;
+    const uint4 r = rec[s];
+    const uint32_t cx = grid_of(texel_of(__uint_as_float(r.x), g.map.wm1), g.rf, g.gw);
+    const uint32_t cy = grid_of(texel_of(__uint_as_float(r.y), g.map.hm1), g.rf, g.gh);
+    out[tag[s] & ~kMovableBit] = cy * g.gw + cx;
 }
 
-__global__ void positions_kernel(const float2* xy, const uint32_t* tag, uint32_t n, float2* out) {
+__global__ void positions_kernel(const uint4* rec, const uint32_t* tag, uint32_t n, float2* out) {
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n) return;
-    out[tag[s] & ~kMovableBit] = xy[s];
+    const uint4 r = rec[s];
+    out[tag[s] & ~kMovableBit] = make_float2(__uint_as_float(r.x), __uint_as_float(r.y));
 }
 
 }  // namespace
@@ -170,10 +233,16 @@ void launch_scatter(const ScatterArgs& a, cudaStream_t s) {
     scatter_kernel<<<div_up(a.n, 256), 256, 0, s>>>(a);
 }
 
-void launch_unsort_records(const float2* xy, const uint32_t* tag, const uint32_t* edge_ids, uint32_t n,
+size_t position_prefix_scratch(uint32_t n) { return scan_scratch_elems(n); }
+
+void launch_position_prefix(const uint4* rec, uint32_t n, LL2* prefix, LL2* scratch, cudaStream_t s) {
+    exclusive_scan<uint4, LL2>(rec, prefix, n, scratch, s);
+}
+
+void launch_unsort_records(const uint4* rec, const uint32_t* tag, const uint32_t* edge_ids, uint32_t n,
                            uint32_t* records, cudaStream_t s) {
     if (n == 0) return;
-    unsort_records_kernel<<<div_up(n, 256), 256, 0, s>>>(xy, tag, edge_ids, n, records);
+    unsort_records_kernel<<<div_up(n, 256), 256, 0, s>>>(rec, tag, edge_ids, n, records);
 }
 
 void launch_unsort_u32(const uint32_t* values, const uint32_t* tag, uint32_t n, uint32_t* out, cudaStream_t s) {
@@ -187,15 +256,15 @@ void launch_records_from_sample_order(const float2* xy, const uint32_t* edge_ids
     records_kernel<<<div_up(n, 256), 256, 0, s>>>(xy, edge_ids, n, records);
 }
 
-void launch_grid_cells(const float2* xy, const uint32_t* tag, uint32_t n, const Grid& g, uint32_t* out,
+void launch_grid_cells(const uint4* rec, const uint32_t* tag, uint32_t n, const Grid& g, uint32_t* out,
                        cudaStream_t s) {
     if (n == 0) return;
-    grid_cells_kernel<<<div_up(n, 256), 256, 0, s>>>(xy, tag, n, g, out);
+    grid_cells_kernel<<<div_up(n, 256), 256, 0, s>>>(rec, tag, n, g, out);
 }
 
-void launch_positions_from_slots(const float2* xy, const uint32_t* tag, uint32_t n, float2* out, cudaStream_t s) {
+void launch_positions_from_slots(const uint4* rec, const uint32_t* tag, uint32_t n, float2* out, cudaStream_t s) {
     if (n == 0) return;
-    positions_kernel<<<div_up(n, 256), 256, 0, s>>>(xy, tag, n, out);
+    positions_kernel<<<div_up(n, 256), 256, 0, s>>>(rec, tag, n, out);
 }
 
 }  // namespace bt

@@ -5,6 +5,7 @@
 #include <stdint.h>
 
 #include "common.cuh"
+#include "scan.cuh"
 
 namespace bt {
 
@@ -68,11 +69,20 @@ void launch_blur_vertical(const float* in, float* out, uint32_t w, uint32_t h, c
 void launch_normalize(const float* in, const uint32_t* peak, float* out, size_t n, cudaStream_t s);
 
 // ---- neighbour grid and mean (grid.cu) ----
+// Slot-order sample record: {f32 x bits, f32 y bits, Qx + 2^30, Qy + 2^30}
+// with Q(v) = round-half-even(v * 2^30), so the biased values are unsigned.
+constexpr uint32_t kFixedBias = 1u << 30;
+
+enum SearchMode : int {
+    kSearchInterior = 0,   // interior search cells from the prefix sums, boundary ring tested exactly
+    kSearchScanAll = 1,    // every sample of the candidate search cells tested exactly
+};
+
 struct MeanArgs {
-    const float2* xy;        // slot order (sorted by search cell)
-    const int2* q;           // fixed-point positions, slot order
+    const uint4* rec;        // slot order (sorted by search cell)
     const uint32_t* tag;     // sample index | movable bit, slot order
     const uint32_t* cell_start;
+    const LL2* prefix;       // exclusive prefix of the biased fixed-point positions, slots + 1
     float2* out_xy;          // new positions, same slot order
     uint32_t* out_tag;
     uint32_t* out_cell;      // search cell of the new position
@@ -81,6 +91,7 @@ struct MeanArgs {
     uint32_t* neighbors;     // |N(p)| per slot (nullptr = off)
     uint32_t n;
     Grid g;
+    int mode;                // SearchMode
 };
 void launch_neighbor_mean(const MeanArgs& a, cudaStream_t s);
 
@@ -90,24 +101,26 @@ struct ScatterArgs {
     const uint32_t* cell;
     const uint32_t* cell_start;
     uint32_t* hist;          // counted down to zero
-    float2* out_xy;
-    int2* out_q;
+    uint4* out_rec;
     uint32_t* out_tag;
     uint32_t n;
     uint32_t cells;          // search cells
     uint32_t* status;        // bit 3 (value 8): inconsistent binning input
 };
 void launch_scatter(const ScatterArgs& a, cudaStream_t s);
+// prefix[s] = sum of the biased fixed-point positions of slots < s.
+void launch_position_prefix(const uint4* rec, uint32_t n, LL2* prefix, LL2* scratch, cudaStream_t s);
+size_t position_prefix_scratch(uint32_t n);
 
 // Sample-order records {x, y, edge_id} from slot order.
-void launch_unsort_records(const float2* xy, const uint32_t* tag, const uint32_t* edge_ids, uint32_t n,
+void launch_unsort_records(const uint4* rec, const uint32_t* tag, const uint32_t* edge_ids, uint32_t n,
                            uint32_t* records, cudaStream_t s);
 void launch_unsort_u32(const uint32_t* values, const uint32_t* tag, uint32_t n, uint32_t* out, cudaStream_t s);
 void launch_records_from_sample_order(const float2* xy, const uint32_t* edge_ids, uint32_t n, uint32_t* records,
                                       cudaStream_t s);
-void launch_grid_cells(const float2* xy, const uint32_t* tag, uint32_t n, const Grid& g, uint32_t* out,
+void launch_grid_cells(const uint4* rec, const uint32_t* tag, uint32_t n, const Grid& g, uint32_t* out,
                        cudaStream_t s);
-void launch_positions_from_slots(const float2* xy, const uint32_t* tag, uint32_t n, float2* out, cudaStream_t s);
+void launch_positions_from_slots(const uint4* rec, const uint32_t* tag, uint32_t n, float2* out, cudaStream_t s);
 
 // ---- distortion (distortion.cu) ----
 // Per-edge squared_integral of original vs current (sample order); status bit

@@ -59,6 +59,10 @@ __device__ __forceinline__ LL2 shfl_down<LL2>(LL2 v, int o) {
 __device__ __forceinline__ uint32_t widen(uint32_t v, uint32_t*) { return v; }
 __device__ __forceinline__ unsigned long long widen(unsigned long long v, unsigned long long*) { return v; }
 __device__ __forceinline__ LL2 widen(int2 v, LL2*) { return LL2{v.x, v.y}; }
+// Slot record {x, y, biased Qx, biased Qy}: the fixed-point half.
+__device__ __forceinline__ LL2 widen(uint4 v, LL2*) {
+    return LL2{static_cast<long long>(v.z), static_cast<long long>(v.w)};
+}
 __device__ __forceinline__ LL2 widen(LL2 v, LL2*) { return v; }
 
 template <typename T>

@@ -63,7 +63,9 @@ typedef struct bt_options {
     uint32_t use_graphs;            /* capture the iteration in a CUDA graph (1 = on, default) */
     uint32_t timing;                /* record per-stage CUDA-event timings */
     uint32_t record_neighbors;      /* keep |N(p)| of the last iteration for bt_read_neighbors */
-    uint32_t reserved[7];
+    uint32_t search_mode;           /* 0: interior search cells from prefix sums, boundary tested
+                                       sample by sample; 1: every candidate tested (same results) */
+    uint32_t reserved[6];
 } bt_options;
 
 typedef struct bt_info {

@@ -162,6 +162,32 @@ def test_search_cell_size_does_not_change_results(oracle, fine):
     check_neighbors(gpu, ora)
 
 
+@pytest.mark.parametrize("mode", [0, 1])
+def test_search_modes_match_oracle(oracle, mode):
+    # Interior cells from prefix sums (0) and testing every candidate (1)
+    # enumerate the same N(p) and give identical sums.
+    w = synthetic.mid()
+    gpu, ora = pair(oracle, w.xy, w.starts, opts_for(w, search_mode=mode))
+    gpu.iterate(2)
+    ora.iterate(2)
+    check_points(gpu, ora)
+    check_neighbors(gpu, ora)
+
+
+@pytest.mark.parametrize("radius,size", [(40, 1024), (33, 1600), (1, 512)])
+def test_interior_bounds_at_other_radii(oracle, radius, size):
+    # Large radii stress the conservative interior bounds; radius 1 has one
+    # search cell per grid cell.
+    w = synthetic.mid()
+    o = bt.Options(width=size, height=size, neighbor_radius=radius, sample_spacing=w.spacing,
+                   blur_sigma=w.sigma, record_neighbors=True)
+    gpu, ora = pair(oracle, w.xy, w.starts, o)
+    gpu.iterate(2)
+    ora.iterate(2)
+    check_points(gpu, ora)
+    check_neighbors(gpu, ora)
+
+
 def test_graphs_and_direct_launches_agree():
     w = synthetic.small()
     out = []
