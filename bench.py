@@ -181,11 +181,11 @@ def profile_traffic():
         return None
 
 
-def scan_launches(n: int) -> int:
-    tile = 2048
+def scan_launches(n: int, tile: int = 1024) -> int:
+    """Launches of the cell-table scan (1024 cells per tile)."""
     if n <= tile:
         return 1
-    return 2 + scan_launches((n + tile - 1) // tile)
+    return 2 + scan_launches((n + tile - 1) // tile, tile)
 
 
 def workload(edges: int):

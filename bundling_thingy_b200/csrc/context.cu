@@ -65,8 +65,8 @@ struct bt_ctx {
 
     DevBuf cp, starts, packed, offsets, scan64, edges, paths, totals, status;
     DevBuf edge_ids, segments, tmp_xy, tmp_tag, tmp_cell, neighbors, baseline, current;
-    DevBuf sorted_rec[2], sorted_tag[2], prefix, prefix_scratch;
-    DevBuf hist, cell_start, scan32;
+    DevBuf sorted_rec[2], sorted_tag[2];
+    DevBuf hist, cellsum, cell_start, cell_prefix, table_scratch;
     DevBuf counts, himg, vimg, norm, peak;
     DevBuf records, integrals;
     unsigned long long* h_totals = nullptr;   // pinned
@@ -236,11 +236,12 @@ bt_status enqueue_density(bt_ctx* c, uint32_t pass) {
     return BT_OK;
 }
 
-// Scan of the search-cell populations and the scatter into slot order `dst`.
+// Cell table of the search-cell populations and sums, then the scatter into
+// slot order `dst`.
 void enqueue_binning(bt_ctx* c, int dst) {
     stage_begin(c, "graph.grid_scan");
-    bt::exclusive_scan<uint32_t, uint32_t>(c->hist.as<uint32_t>(), c->cell_start.as<uint32_t>(), c->cells,
-                                           c->scan32.as<uint32_t>(), c->stream);
+    bt::launch_cell_table(c->hist.as<uint32_t>(), c->cellsum.as<bt::LL2>(), c->cells, c->cell_start.as<uint32_t>(),
+                          c->cell_prefix.as<bt::LL2>(), c->table_scratch.as<bt::LL3>(), c->stream);
     stage_end(c);
     stage_begin(c, "graph.grid_scatter");
     bt::ScatterArgs s{};
@@ -256,12 +257,6 @@ void enqueue_binning(bt_ctx* c, int dst) {
     s.status = c->status.as<uint32_t>();
     bt::launch_scatter(s, c->stream);
     stage_end(c);
-    if (c->opt.search_mode == bt::kSearchInterior) {
-        stage_begin(c, "graph.position_prefix");
-        bt::launch_position_prefix(c->sorted_rec[dst].as<uint4>(), c->samples, c->prefix.as<bt::LL2>(),
-                                   c->prefix_scratch.as<bt::LL2>(), c->stream);
-        stage_end(c);
-    }
 }
 
 // One Gpu::iterate (gpu.rs:527-553) starting from slot order `src`.
@@ -275,12 +270,13 @@ bt_status enqueue_iteration(bt_ctx* c, int src, uint32_t pass) {
     m.rec = c->sorted_rec[src].as<uint4>();
     m.tag = c->sorted_tag[src].as<uint32_t>();
     m.cell_start = c->cell_start.as<uint32_t>();
-    m.prefix = c->prefix.as<bt::LL2>();
+    m.cell_prefix = c->cell_prefix.as<bt::LL2>();
     m.mode = static_cast<int>(c->opt.search_mode);
     m.out_xy = c->tmp_xy.as<float2>();
     m.out_tag = c->tmp_tag.as<uint32_t>();
     m.out_cell = c->tmp_cell.as<uint32_t>();
     m.hist = c->hist.as<uint32_t>();
+    m.cellsum = c->cellsum.as<bt::LL2>();
     m.counts = c->accumulate ? c->counts.as<uint32_t>() : nullptr;
     m.neighbors = c->opt.record_neighbors ? c->neighbors.as<uint32_t>() : nullptr;
     m.n = c->samples;
@@ -389,7 +385,9 @@ bt_status bt_create(const bt_options* options, bt_ctx** out) {
         g.rf = static_cast<float>(r);
         g.gw = (W + r - 1) / r;
         g.gh = (H + r - 1) / r;
-        g.k = options->fine_cells ? options->fine_cells : r;   // search cells of about one texel
+        // Search cells of about two texels by default (the fastest side on the
+        // large workload among 1, 2, 4 and 8 texels).
+        g.k = options->fine_cells ? options->fine_cells : std::max(1u, r / 2u);
         g.inv_s = static_cast<float>(g.k) / g.rf;
         g.s = g.rf / static_cast<float>(g.k);
         g.fw = g.gw * g.k;
@@ -405,7 +403,12 @@ bt_status bt_create(const bt_options* options, bt_ctx** out) {
         c->grid_bytes_ref = reference_grid_bytes(W, H, r);
         if (bt_status s = ensure(c, c->hist, c->cells * 4)) return bail(s);
         if (bt_status s = ensure(c, c->cell_start, (c->cells + 1) * 4)) return bail(s);
-        if (bt_status s = ensure(c, c->scan32, bt::scan_scratch_elems(c->cells) * 4)) return bail(s);
+        if (bt_status s = ensure(c, c->cellsum, c->cells * sizeof(bt::LL2))) return bail(s);
+        if (bt_status s = ensure(c, c->cell_prefix, (c->cells + 1) * sizeof(bt::LL2))) return bail(s);
+        if (bt_status s = ensure(c, c->table_scratch, bt::cell_table_scratch(c->cells) * sizeof(bt::LL3)))
+            return bail(s);
+        if ((e = cudaMemsetAsync(c->cellsum.p, 0, c->cells * sizeof(bt::LL2), c->stream)) != cudaSuccess)
+            return bail(cuda_fail(c, e, "cudaMemset"));
         if ((e = cudaMemsetAsync(c->hist.p, 0, c->cells * 4, c->stream)) != cudaSuccess)
             return bail(cuda_fail(c, e, "cudaMemset"));
     }
@@ -432,8 +435,8 @@ void bt_destroy(bt_ctx* c) {
     DevBuf* bufs[] = {&c->cp, &c->starts, &c->packed, &c->offsets, &c->scan64, &c->edges, &c->paths, &c->totals,
                       &c->status, &c->edge_ids, &c->segments, &c->tmp_xy, &c->tmp_tag, &c->tmp_cell,
                       &c->neighbors, &c->baseline, &c->current, &c->sorted_rec[0], &c->sorted_rec[1],
-                      &c->prefix, &c->prefix_scratch, &c->sorted_tag[0], &c->sorted_tag[1], &c->hist,
-                      &c->cell_start, &c->scan32, &c->counts, &c->himg, &c->vimg, &c->norm, &c->peak,
+                      &c->cellsum, &c->cell_prefix, &c->sorted_tag[0], &c->sorted_tag[1], &c->hist,
+                      &c->cell_start, &c->table_scratch, &c->counts, &c->himg, &c->vimg, &c->norm, &c->peak,
                       &c->records, &c->integrals};
     for (DevBuf* b : bufs) release(*b);
     for (StageRec& r : c->stage_pool) {
@@ -500,7 +503,7 @@ bt_status bt_upload(bt_ctx* c, const float* xy, uint32_t n_points, const uint32_
     if (bt_status s = ensure(c, c->starts, 4ull * n_starts)) return s;
     if (bt_status s = ensure(c, c->packed, 8ull * E)) return s;
     if (bt_status s = ensure(c, c->offsets, 8ull * (E + 1))) return s;
-    if (bt_status s = ensure(c, c->scan64, 8ull * bt::scan_scratch_elems(E))) return s;
+    if (bt_status s = ensure(c, c->scan64, 8ull * bt::scan_scratch_elems<unsigned long long>(E))) return s;
     if (bt_status s = ensure(c, c->edges, 16ull * E)) return s;
     if (bt_status s = ensure(c, c->paths, 12ull * E)) return s;
     BT_CUDA(c, cudaMemcpyAsync(c->cp.p, xy, 8ull * n_points, cudaMemcpyHostToDevice, c->stream));
@@ -537,9 +540,8 @@ bt_status bt_upload(bt_ctx* c, const float* xy, uint32_t n_points, const uint32_
     const uint32_t segs = static_cast<uint32_t>(total - drawn);
 
     stage_begin(c, "graph.emit");
-    bt::exclusive_scan<unsigned long long, unsigned long long>(c->packed.as<unsigned long long>(),
-                                                               c->offsets.as<unsigned long long>(), E,
-                                                               c->scan64.as<unsigned long long>(), c->stream);
+    bt::exclusive_scan<unsigned long long>(c->packed.as<unsigned long long>(), c->offsets.as<unsigned long long>(), E,
+                                           c->scan64.as<unsigned long long>(), c->stream);
     bt::launch_paths_from_scan(c->packed.as<unsigned long long>(), c->offsets.as<unsigned long long>(), E,
                                c->paths.as<bt::PathRec>(), c->stream);
     if (bt_status s = ensure(c, c->edge_ids, 4ull * N)) return s;
@@ -552,14 +554,10 @@ bt_status bt_upload(bt_ctx* c, const float* xy, uint32_t n_points, const uint32_
             if (bt_status s = ensure(c, c->sorted_rec[b], 16ull * N)) return s;
             if (bt_status s = ensure(c, c->sorted_tag[b], 4ull * N)) return s;
         }
-        if (c->opt.search_mode == bt::kSearchInterior) {
-            if (bt_status s = ensure(c, c->prefix, sizeof(bt::LL2) * (N + 1ull))) return s;
-            if (bt_status s = ensure(c, c->prefix_scratch, sizeof(bt::LL2) * bt::position_prefix_scratch(N)))
-                return s;
-        }
         if (c->opt.record_neighbors)
             if (bt_status s = ensure(c, c->neighbors, 4ull * N)) return s;
         BT_CUDA(c, cudaMemsetAsync(c->hist.p, 0, c->cells * 4, c->stream));
+        BT_CUDA(c, cudaMemsetAsync(c->cellsum.p, 0, c->cells * sizeof(bt::LL2), c->stream));
     }
     if (c->opt.evaluate_distortion)
         if (bt_status s = ensure(c, c->baseline, 8ull * N)) return s;
@@ -584,6 +582,7 @@ bt_status bt_upload(bt_ctx* c, const float* xy, uint32_t n_points, const uint32_
     ea.tag = c->tmp_tag.as<uint32_t>();
     ea.cell = c->tmp_cell.as<uint32_t>();
     ea.hist = c->hist.as<uint32_t>();
+    ea.cellsum = c->cellsum.as<bt::LL2>();
     ea.status = c->status.as<uint32_t>();
     bt::launch_resample_emit(ea, c->stream);
     stage_end(c);

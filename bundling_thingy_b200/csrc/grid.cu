@@ -31,8 +31,10 @@
 namespace bt {
 namespace {
 
-__device__ __forceinline__ int floor_div(float t, float s) { return static_cast<int>(floorf(t / s)); }
-__device__ __forceinline__ int ceil_div(float t, float s) { return static_cast<int>(ceilf(t / s)); }
+// Search-cell index bounds t / s, by the reciprocal: the bounds are
+// conservative by the margin, which exceeds this rounding many times over.
+__device__ __forceinline__ int floor_cell(float t, float inv_s) { return static_cast<int>(floorf(t * inv_s)); }
+__device__ __forceinline__ int ceil_cell(float t, float inv_s) { return static_cast<int>(ceilf(t * inv_s)); }
 
 // Approximate square root (one MUFU op); callers widen its result by a
 // relative 1e-6 plus the margin, far above its error.
@@ -67,11 +69,11 @@ __device__ __forceinline__ void scan_range(const uint4* __restrict__ rec, uint32
 
 __global__ void __launch_bounds__(256) neighbor_mean_kernel(MeanArgs a) {
     const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
-    if (slot >= a.n) return;
+    const bool valid = slot < a.n;
     const Grid& g = a.g;
-    const uint4 me = a.rec[slot];
+    const uint4 me = valid ? a.rec[slot] : make_uint4(0u, 0u, 0u, 0u);
     const float2 p = make_float2(__uint_as_float(me.x), __uint_as_float(me.y));
-    const uint32_t tag = a.tag[slot];
+    const uint32_t tag = valid ? a.tag[slot] : 0u;
     float2 np = p;
     uint32_t count = 0;
     if (tag & kMovableBit) {
@@ -84,8 +86,8 @@ __global__ void __launch_bounds__(256) neighbor_mean_kernel(MeanArgs a) {
         // Candidate circle r + m; certain circle r - m (texels).
         const float R = g.rf + g.margin;
         const float Rin = g.rf - g.margin;
-        const int fy_lo = max(fy_min, floor_div(ty - R, g.s));
-        const int fy_hi = min(fy_max, floor_div(ty + R, g.s));
+        const int fy_lo = max(fy_min, floor_cell(ty - R, g.inv_s));
+        const int fy_hi = min(fy_max, floor_cell(ty + R, g.inv_s));
         const bool interior = a.mode == kSearchInterior;
         const int fw = static_cast<int>(g.fw), fh = static_cast<int>(g.fh);
         const float2 neg_p = make_float2(-p.x, -p.y);
@@ -99,8 +101,8 @@ __global__ void __launch_bounds__(256) neighbor_mean_kernel(MeanArgs a) {
             if (dn > R) continue;
             // f32 rounding of R^2 - dn^2 is below 5e-7 R^2; widen by that.
             const float hout = sqrt_approx(fmaxf(R * R - dn * dn + 5e-7f * R * R, 0.0f)) * 1.000001f + g.margin;
-            const int bx0 = max(fx_min, floor_div(tx - hout, g.s));
-            const int bx1 = min(fx_max, floor_div(tx + hout, g.s));
+            const int bx0 = max(fx_min, floor_cell(tx - hout, g.inv_s));
+            const int bx1 = min(fx_max, floor_cell(tx + hout, g.inv_s));
             if (bx0 > bx1) continue;
             const uint32_t row = static_cast<uint32_t>(fy) * g.fw;
             const uint32_t s0 = a.cell_start[row + bx0];
@@ -114,15 +116,15 @@ __global__ void __launch_bounds__(256) neighbor_mean_kernel(MeanArgs a) {
                     const float h2 = Rin * Rin - far * far - 5e-7f * Rin * Rin;
                     const float hin = sqrt_approx(fmaxf(h2, 0.0f)) * 0.999999f - g.margin;
                     if (hin > 0.0f) {
-                        ix0 = max(ceil_div(tx - hin, g.s), max(bx0, 1));
-                        ix1 = min(floor_div(tx + hin, g.s) - 1, min(bx1, fw - 2));
+                        ix0 = max(ceil_cell(tx - hin, g.inv_s), max(bx0, 1));
+                        ix1 = min(floor_cell(tx + hin, g.inv_s) - 1, min(bx1, fw - 2));
                     }
                 }
             }
             if (ix0 <= ix1) {
                 const uint32_t s1 = a.cell_start[row + ix0];
                 const uint32_t s2 = a.cell_start[row + ix1 + 1];
-                const LL2 lo = a.prefix[s1], hi = a.prefix[s2];
+                const LL2 lo = a.cell_prefix[row + ix0], hi = a.cell_prefix[row + ix1 + 1];
                 acc.sx += static_cast<unsigned long long>(hi.x - lo.x);
                 acc.sy += static_cast<unsigned long long>(hi.y - lo.y);
                 acc.count += s2 - s1;
@@ -140,11 +142,26 @@ __global__ void __launch_bounds__(256) neighbor_mean_kernel(MeanArgs a) {
         np.x = p.x + static_cast<float>(static_cast<double>(dx) / den);
         np.y = p.y + static_cast<float>(static_cast<double>(dy) / den);
     }
+    // The next grid: search cell, population and biased position sum. Lanes
+    // of a warp that land in one cell (neighbours in slot order mostly do)
+    // add their counts and sums once.
+    const uint32_t c = valid ? search_cell(np, g) : 0xFFFFFFFFu;
+    const unsigned peers = __match_any_sync(0xFFFFFFFFu, c);
+    if (!valid) return;
+    const uint32_t qx = biased_fixed(np.x), qy = biased_fixed(np.y);
+    // Group sums in 16-bit halves so each 32-bit reduction cannot overflow.
+    const uint32_t xl = __reduce_add_sync(peers, qx & 0xFFFFu), xh = __reduce_add_sync(peers, qx >> 16);
+    const uint32_t yl = __reduce_add_sync(peers, qy & 0xFFFFu), yh = __reduce_add_sync(peers, qy >> 16);
+    if ((threadIdx.x & 31) == __ffs(peers) - 1) {
+        atomicAdd(&a.hist[c], static_cast<uint32_t>(__popc(peers)));
+        atomicAdd(reinterpret_cast<unsigned long long*>(&a.cellsum[c].x),
+                  (static_cast<unsigned long long>(xh) << 16) + xl);
+        atomicAdd(reinterpret_cast<unsigned long long*>(&a.cellsum[c].y),
+                  (static_cast<unsigned long long>(yh) << 16) + yl);
+    }
     a.out_xy[slot] = np;
     a.out_tag[slot] = tag;
-    const uint32_t c = search_cell(np, g);
     a.out_cell[slot] = c;
-    atomicAdd(&a.hist[c], 1u);
     if (a.counts) {
         uint32_t d;
         if (splat_index(np.x, np.y, g.map, &d)) atomicAdd(&a.counts[d], 1u);
@@ -157,24 +174,32 @@ __global__ void __launch_bounds__(256) neighbor_mean_kernel(MeanArgs a) {
 // the mean's exact sum does not depend on it).
 __global__ void __launch_bounds__(256) scatter_kernel(ScatterArgs a) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.n) return;
-    const uint32_t c = a.cell[i];
+    const bool valid = i < a.n;
+    const uint32_t c = valid ? a.cell[i] : 0xFFFFFFFFu;
+    // Lanes of one warp that share a cell (neighbours in slot order mostly do)
+    // take one reservation and consecutive slots, so their writes coalesce.
+    const unsigned peers = __match_any_sync(0xFFFFFFFFu, c);
+    if (!valid) return;
     // Cell ids and populations are consistent by construction; a failed
     // upload can leave stale entries, which are skipped and flagged.
     if (c >= a.cells) {
         atomicOr(a.status, 8u);
         return;
     }
-    const uint32_t rank = atomicSub(&a.hist[c], 1u);
-    const uint32_t slot = a.cell_start[c] + rank - 1u;
-    if (rank == 0u || slot >= a.n) {
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(peers) - 1;
+    const uint32_t group = __popc(peers);
+    const uint32_t rank = __popc(peers & ((1u << lane) - 1u));
+    uint32_t top = 0;
+    if (lane == leader) top = atomicSub(&a.hist[c], group);
+    top = __shfl_sync(peers, top, leader);
+    const uint32_t slot = a.cell_start[c] + (top - group) + rank;
+    if (top < group || slot >= a.n) {
         atomicOr(a.status, 8u);
         return;
     }
     const float2 p = a.xy[i];
-    const uint32_t qx = static_cast<uint32_t>(__float2int_rn(p.x * kFixedScale)) + kFixedBias;
-    const uint32_t qy = static_cast<uint32_t>(__float2int_rn(p.y * kFixedScale)) + kFixedBias;
-    a.out_rec[slot] = make_uint4(__float_as_uint(p.x), __float_as_uint(p.y), qx, qy);
+    a.out_rec[slot] = make_uint4(__float_as_uint(p.x), __float_as_uint(p.y), biased_fixed(p.x), biased_fixed(p.y));
     a.out_tag[slot] = a.tag[i];
 }
 
@@ -233,10 +258,35 @@ void launch_scatter(const ScatterArgs& a, cudaStream_t s) {
     scatter_kernel<<<div_up(a.n, 256), 256, 0, s>>>(a);
 }
 
-size_t position_prefix_scratch(uint32_t n) { return scan_scratch_elems(n); }
+namespace {
+// Scan input: a cell's population and position sums; the sums are cleared
+// after their last read so the next iteration accumulates from zero.
+struct CellAccSource {
+    const uint32_t* hist;
+    LL2* cellsum;
+    __device__ __forceinline__ LL3 read(size_t j) const {
+        const LL2 s = cellsum[j];
+        return LL3{static_cast<long long>(hist[j]), s.x, s.y};
+    }
+    __device__ __forceinline__ void consume(size_t j) const { cellsum[j] = LL2{0, 0}; }
+};
 
-void launch_position_prefix(const uint4* rec, uint32_t n, LL2* prefix, LL2* scratch, cudaStream_t s) {
-    exclusive_scan<uint4, LL2>(rec, prefix, n, scratch, s);
+struct CellTableSink {
+    uint32_t* cell_start;
+    LL2* cell_prefix;
+    __device__ __forceinline__ void store(size_t j, LL3 v) const {
+        cell_start[j] = static_cast<uint32_t>(v.c);
+        cell_prefix[j] = LL2{v.x, v.y};
+    }
+};
+}  // namespace
+
+size_t cell_table_scratch(size_t cells) { return scan_scratch_elems<LL3>(cells); }
+int cell_table_launches(size_t cells) { return scan_launch_count<LL3>(cells); }
+
+void launch_cell_table(const uint32_t* hist, LL2* cellsum, size_t cells, uint32_t* cell_start, LL2* cell_prefix,
+                       LL3* scratch, cudaStream_t s) {
+    exclusive_scan_with<LL3>(CellAccSource{hist, cellsum}, CellTableSink{cell_start, cell_prefix}, cells, scratch, s);
 }
 
 void launch_unsort_records(const uint4* rec, const uint32_t* tag, const uint32_t* edge_ids, uint32_t n,

@@ -51,6 +51,7 @@ struct ResampleEmitArgs {
     uint32_t* tag;           // sample index | movable bit, sample order
     uint32_t* cell;          // search cell of each sample
     uint32_t* hist;          // search-cell populations
+    LL2* cellsum;            // search-cell sums of the biased fixed-point positions
     uint32_t* status;        // bit 1: count/emit mismatch
 };
 void launch_resample_emit(const ResampleEmitArgs& a, cudaStream_t s);
@@ -73,6 +74,16 @@ void launch_normalize(const float* in, const uint32_t* peak, float* out, size_t 
 // with Q(v) = round-half-even(v * 2^30), so the biased values are unsigned.
 constexpr uint32_t kFixedBias = 1u << 30;
 
+__device__ __forceinline__ uint32_t biased_fixed(float v) {
+    return static_cast<uint32_t>(__float2int_rn(v * kFixedScale)) + kFixedBias;
+}
+
+// Adds a sample's biased fixed-point position to its cell's sums.
+__device__ __forceinline__ void add_cell_sum(LL2* cellsum, uint32_t c, uint32_t qx, uint32_t qy) {
+    atomicAdd(reinterpret_cast<unsigned long long*>(&cellsum[c].x), static_cast<unsigned long long>(qx));
+    atomicAdd(reinterpret_cast<unsigned long long*>(&cellsum[c].y), static_cast<unsigned long long>(qy));
+}
+
 enum SearchMode : int {
     kSearchInterior = 0,   // interior search cells from the prefix sums, boundary ring tested exactly
     kSearchScanAll = 1,    // every sample of the candidate search cells tested exactly
@@ -81,12 +92,13 @@ enum SearchMode : int {
 struct MeanArgs {
     const uint4* rec;        // slot order (sorted by search cell)
     const uint32_t* tag;     // sample index | movable bit, slot order
-    const uint32_t* cell_start;
-    const LL2* prefix;       // exclusive prefix of the biased fixed-point positions, slots + 1
+    const uint32_t* cell_start;   // cell table: first slot of each search cell (cells + 1)
+    const LL2* cell_prefix;  // cell table: sum of the biased positions of all earlier slots (cells + 1)
     float2* out_xy;          // new positions, same slot order
     uint32_t* out_tag;
     uint32_t* out_cell;      // search cell of the new position
     uint32_t* hist;          // populations of the next grid
+    LL2* cellsum;            // biased position sums of the next grid
     uint32_t* counts;        // density splat (nullptr = off)
     uint32_t* neighbors;     // |N(p)| per slot (nullptr = off)
     uint32_t n;
@@ -94,6 +106,13 @@ struct MeanArgs {
     int mode;                // SearchMode
 };
 void launch_neighbor_mean(const MeanArgs& a, cudaStream_t s);
+
+// Cell table of the next slot order from the populations and sums (the sums
+// are cleared for reuse; the populations stay for the scatter's count-down).
+void launch_cell_table(const uint32_t* hist, LL2* cellsum, size_t cells, uint32_t* cell_start, LL2* cell_prefix,
+                       LL3* scratch, cudaStream_t s);
+size_t cell_table_scratch(size_t cells);
+int cell_table_launches(size_t cells);
 
 struct ScatterArgs {
     const float2* xy;
@@ -108,9 +127,6 @@ struct ScatterArgs {
     uint32_t* status;        // bit 3 (value 8): inconsistent binning input
 };
 void launch_scatter(const ScatterArgs& a, cudaStream_t s);
-// prefix[s] = sum of the biased fixed-point positions of slots < s.
-void launch_position_prefix(const uint4* rec, uint32_t n, LL2* prefix, LL2* scratch, cudaStream_t s);
-size_t position_prefix_scratch(uint32_t n);
 
 // Sample-order records {x, y, edge_id} from slot order.
 void launch_unsort_records(const uint4* rec, const uint32_t* tag, const uint32_t* edge_ids, uint32_t n,

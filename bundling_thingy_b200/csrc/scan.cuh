@@ -4,6 +4,10 @@
 // (resampling.wgsl:151,157 and spatial_grid.wgsl:110,119): offsets come out in
 // index order. Three launches per level; levels recurse on the block sums.
 // Sums are integers, so any association order gives the same result.
+//
+// A scan reads through a Source (read(j) gives element j; consume(j) runs
+// after the last read of j, e.g. to clear an accumulator for its next use)
+// and writes through a Sink (store(j, prefix)); plain arrays are the default.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -14,8 +18,6 @@
 namespace bt {
 
 constexpr int kScanBlock = 256;
-constexpr int kScanItems = 8;
-constexpr size_t kScanTile = static_cast<size_t>(kScanBlock) * kScanItems;
 
 // Pair of 64-bit sums (fixed-point x and y).
 struct LL2 {
@@ -29,6 +31,20 @@ __host__ __device__ __forceinline__ LL2& operator+=(LL2& a, LL2 b) {
     return a;
 }
 
+// Count and fixed-point sums of a search cell; its exclusive prefix over the
+// cells is the cell table {first slot, sum of the positions before it}.
+struct LL3 {
+    long long c, x, y;
+};
+__host__ __device__ __forceinline__ LL3 operator+(LL3 a, LL3 b) { return LL3{a.c + b.c, a.x + b.x, a.y + b.y}; }
+__host__ __device__ __forceinline__ LL3 operator-(LL3 a, LL3 b) { return LL3{a.c - b.c, a.x - b.x, a.y - b.y}; }
+__host__ __device__ __forceinline__ LL3& operator+=(LL3& a, LL3 b) {
+    a.c += b.c;
+    a.x += b.x;
+    a.y += b.y;
+    return a;
+}
+
 template <typename T>
 __device__ __forceinline__ T zero() {
     return T(0);
@@ -36,6 +52,10 @@ __device__ __forceinline__ T zero() {
 template <>
 __device__ __forceinline__ LL2 zero<LL2>() {
     return LL2{0, 0};
+}
+template <>
+__device__ __forceinline__ LL3 zero<LL3>() {
+    return LL3{0, 0, 0};
 }
 
 template <typename T>
@@ -46,6 +66,11 @@ template <>
 __device__ __forceinline__ LL2 shfl_up<LL2>(LL2 v, int o) {
     return LL2{__shfl_up_sync(0xFFFFFFFFu, v.x, o), __shfl_up_sync(0xFFFFFFFFu, v.y, o)};
 }
+template <>
+__device__ __forceinline__ LL3 shfl_up<LL3>(LL3 v, int o) {
+    return LL3{__shfl_up_sync(0xFFFFFFFFu, v.c, o), __shfl_up_sync(0xFFFFFFFFu, v.x, o),
+               __shfl_up_sync(0xFFFFFFFFu, v.y, o)};
+}
 template <typename T>
 __device__ __forceinline__ T shfl_down(T v, int o) {
     return __shfl_down_sync(0xFFFFFFFFu, v, o);
@@ -54,16 +79,34 @@ template <>
 __device__ __forceinline__ LL2 shfl_down<LL2>(LL2 v, int o) {
     return LL2{__shfl_down_sync(0xFFFFFFFFu, v.x, o), __shfl_down_sync(0xFFFFFFFFu, v.y, o)};
 }
-
-// Input conversions.
-__device__ __forceinline__ uint32_t widen(uint32_t v, uint32_t*) { return v; }
-__device__ __forceinline__ unsigned long long widen(unsigned long long v, unsigned long long*) { return v; }
-__device__ __forceinline__ LL2 widen(int2 v, LL2*) { return LL2{v.x, v.y}; }
-// Slot record {x, y, biased Qx, biased Qy}: the fixed-point half.
-__device__ __forceinline__ LL2 widen(uint4 v, LL2*) {
-    return LL2{static_cast<long long>(v.z), static_cast<long long>(v.w)};
+template <>
+__device__ __forceinline__ LL3 shfl_down<LL3>(LL3 v, int o) {
+    return LL3{__shfl_down_sync(0xFFFFFFFFu, v.c, o), __shfl_down_sync(0xFFFFFFFFu, v.x, o),
+               __shfl_down_sync(0xFFFFFFFFu, v.y, o)};
 }
-__device__ __forceinline__ LL2 widen(LL2 v, LL2*) { return v; }
+
+// Items per thread: tiles of 2048 elements up to 16 bytes, 1024 above.
+template <typename T>
+__host__ __device__ constexpr int scan_items() {
+    return sizeof(T) <= 16 ? 8 : 4;
+}
+template <typename T>
+__host__ __device__ constexpr size_t scan_tile() {
+    return static_cast<size_t>(kScanBlock) * scan_items<T>();
+}
+
+template <typename T>
+struct ArraySource {
+    const T* p;
+    __device__ __forceinline__ T read(size_t j) const { return p[j]; }
+    __device__ __forceinline__ void consume(size_t) const {}
+};
+
+template <typename T>
+struct ArraySink {
+    T* p;
+    __device__ __forceinline__ void store(size_t j, T v) const { p[j] = v; }
+};
 
 template <typename T>
 __device__ __forceinline__ T block_sum(T v, T* warp_sums) {
@@ -114,39 +157,47 @@ __device__ __forceinline__ T block_exclusive(T v, T* warp_sums, T* total) {
     return prefix;
 }
 
-template <typename In, typename T>
-__global__ void __launch_bounds__(kScanBlock) scan_reduce_kernel(const In* in, size_t n, T* sums) {
+template <typename T, typename Source>
+__global__ void __launch_bounds__(kScanBlock) scan_reduce_kernel(Source in, size_t n, T* sums) {
     __shared__ T warp_sums[kScanBlock / 32 + 1];
-    const size_t base = static_cast<size_t>(blockIdx.x) * kScanTile;
+    constexpr int kItems = scan_items<T>();
+    const size_t base = static_cast<size_t>(blockIdx.x) * scan_tile<T>();
     T acc = zero<T>();
 #pragma unroll
-    for (int i = 0; i < kScanItems; ++i) {
+    for (int i = 0; i < kItems; ++i) {
         size_t j = base + static_cast<size_t>(i) * kScanBlock + threadIdx.x;
-        if (j < n) acc += widen(in[j], static_cast<T*>(nullptr));
+        if (j < n) acc += in.read(j);
     }
     acc = block_sum(acc, warp_sums);
     if (threadIdx.x == 0) sums[blockIdx.x] = acc;
 }
 
 // out[j] = offsets[block] + sum(in[tile start .. j)); out[n] = total.
-template <typename In, typename T>
-__global__ void __launch_bounds__(kScanBlock) scan_apply_kernel(const In* in, size_t n, const T* offsets, T* out) {
-    __shared__ T tile[kScanTile + kScanTile / 32];
+template <typename T, typename Source, typename Sink>
+__global__ void __launch_bounds__(kScanBlock) scan_apply_kernel(Source in, size_t n, const T* offsets, Sink out) {
+    constexpr int kItems = scan_items<T>();
+    constexpr int kTile = kScanBlock * kItems;
+    __shared__ T tile[kTile + kTile / 32];
     __shared__ T warp_sums[kScanBlock / 32 + 1];
-    const size_t base = static_cast<size_t>(blockIdx.x) * kScanTile;
+    const size_t base = static_cast<size_t>(blockIdx.x) * kTile;
     auto pad = [](int i) { return i + (i >> 5); };
 #pragma unroll
-    for (int i = 0; i < kScanItems; ++i) {
+    for (int i = 0; i < kItems; ++i) {
         int t = i * kScanBlock + threadIdx.x;
         size_t j = base + t;
-        tile[pad(t)] = j < n ? widen(in[j], static_cast<T*>(nullptr)) : zero<T>();
+        if (j < n) {
+            tile[pad(t)] = in.read(j);
+            in.consume(j);
+        } else {
+            tile[pad(t)] = zero<T>();
+        }
     }
     __syncthreads();
-    T local[kScanItems];
+    T local[kItems];
     T sum = zero<T>();
 #pragma unroll
-    for (int i = 0; i < kScanItems; ++i) {
-        local[i] = tile[pad(threadIdx.x * kScanItems + i)];
+    for (int i = 0; i < kItems; ++i) {
+        local[i] = tile[pad(threadIdx.x * kItems + i)];
         sum += local[i];
     }
     T block_total;
@@ -154,54 +205,59 @@ __global__ void __launch_bounds__(kScanBlock) scan_apply_kernel(const In* in, si
     const T offset = offsets ? offsets[blockIdx.x] : zero<T>();
     prefix += offset;
 #pragma unroll
-    for (int i = 0; i < kScanItems; ++i) {
-        tile[pad(threadIdx.x * kScanItems + i)] = prefix;
+    for (int i = 0; i < kItems; ++i) {
+        tile[pad(threadIdx.x * kItems + i)] = prefix;
         prefix += local[i];
     }
     __syncthreads();
 #pragma unroll
-    for (int i = 0; i < kScanItems; ++i) {
+    for (int i = 0; i < kItems; ++i) {
         int t = i * kScanBlock + threadIdx.x;
         size_t j = base + t;
-        if (j < n) out[j] = tile[pad(t)];
+        if (j < n) out.store(j, tile[pad(t)]);
     }
-    if (threadIdx.x == 0 && base + kScanTile >= n) out[n] = offset + block_total;
+    if (threadIdx.x == 0 && base + kTile >= n) out.store(n, offset + block_total);
 }
 
 // Each level keeps its block sums and their scan (blocks + 1 entries each).
+template <typename T>
 inline size_t scan_scratch_elems(size_t n) {
     size_t total = 0;
-    while (n > kScanTile) {
-        n = (n + kScanTile - 1) / kScanTile;
+    while (n > scan_tile<T>()) {
+        n = (n + scan_tile<T>() - 1) / scan_tile<T>();
         total += 2 * (n + 1);
     }
     return total + 1;
 }
 
-// Number of kernel launches of exclusive_scan for n inputs.
+// Number of kernel launches of a scan of n elements of T.
+template <typename T>
 inline int scan_launch_count(size_t n) {
     if (n == 0) return 0;
-    if (n <= kScanTile) return 1;
-    return 2 + scan_launch_count((n + kScanTile - 1) / kScanTile);
+    if (n <= scan_tile<T>()) return 1;
+    return 2 + scan_launch_count<T>((n + scan_tile<T>() - 1) / scan_tile<T>());
 }
 
-// out has n + 1 elements; out[n] receives the total. in and out may not alias.
-template <typename In, typename T>
-void exclusive_scan(const In* in, T* out, size_t n, T* scratch, cudaStream_t stream) {
-    if (n == 0) {
-        cudaMemsetAsync(out, 0, sizeof(T), stream);
-        return;
-    }
-    const size_t blocks = (n + kScanTile - 1) / kScanTile;
-    if (blocks == 1) {
-        scan_apply_kernel<In, T><<<1, kScanBlock, 0, stream>>>(in, n, nullptr, out);
+// Exclusive scan of n elements; the sink receives n + 1 values (the last is
+// the total). Source and sink must not alias.
+template <typename T, typename Source, typename Sink>
+void exclusive_scan_with(Source in, Sink out, size_t n, T* scratch, cudaStream_t stream) {
+    const size_t blocks = (n + scan_tile<T>() - 1) / scan_tile<T>();
+    if (blocks <= 1) {
+        scan_apply_kernel<T, Source, Sink><<<1, kScanBlock, 0, stream>>>(in, n, nullptr, out);
         return;
     }
     T* sums = scratch;              // blocks + 1 entries
     T* rest = scratch + blocks + 1;
-    scan_reduce_kernel<In, T><<<static_cast<unsigned>(blocks), kScanBlock, 0, stream>>>(in, n, sums);
-    exclusive_scan<T, T>(sums, rest, blocks, rest + blocks + 1, stream);
-    scan_apply_kernel<In, T><<<static_cast<unsigned>(blocks), kScanBlock, 0, stream>>>(in, n, rest, out);
+    scan_reduce_kernel<T, Source><<<static_cast<unsigned>(blocks), kScanBlock, 0, stream>>>(in, n, sums);
+    exclusive_scan_with<T>(ArraySource<T>{sums}, ArraySink<T>{rest}, blocks, rest + blocks + 1, stream);
+    scan_apply_kernel<T, Source, Sink><<<static_cast<unsigned>(blocks), kScanBlock, 0, stream>>>(in, n, rest, out);
+}
+
+// Plain arrays: out has n + 1 elements.
+template <typename T>
+void exclusive_scan(const T* in, T* out, size_t n, T* scratch, cudaStream_t stream) {
+    exclusive_scan_with<T>(ArraySource<T>{in}, ArraySink<T>{out}, n, scratch, stream);
 }
 
 }  // namespace bt
