@@ -171,14 +171,17 @@ def measured_peak_hbm():
 
 
 def profile_traffic():
-    """DRAM bytes per launch of the neighbour-mean kernel from the committed
-    ncu summary (profiles/neighbor_mean_large.json), or None."""
-    path = os.path.join(ROOT, "profiles", "neighbor_mean_large.json")
+    """DRAM bytes (read + write) per launch of the neighbour-mean kernel from
+    the committed ncu summary (profiles/neighbor_mean_large.md), or None."""
+    path = os.path.join(ROOT, "profiles", "neighbor_mean_large.md")
     try:
         with open(path) as f:
-            return json.load(f).get("dram_bytes_per_launch")
+            for line in f:
+                if line.startswith("dram_bytes_per_launch:"):
+                    return int(line.split(":", 1)[1])
     except (OSError, ValueError):
-        return None
+        pass
+    return None
 
 
 def scan_launches(n: int, tile: int = 1024) -> int:
