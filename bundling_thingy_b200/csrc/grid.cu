@@ -67,7 +67,9 @@ __device__ __forceinline__ void scan_range(const uint4* __restrict__ rec, uint32
     }
 }
 
-__global__ void __launch_bounds__(256) neighbor_mean_kernel(MeanArgs a) {
+// Six resident 256-thread CTAs per SM (at most 42 registers) hide more of
+// the cell-table and record load latency than five.
+__global__ void __launch_bounds__(256, 6) neighbor_mean_kernel(MeanArgs a) {
     const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
     const bool valid = slot < a.n;
     const Grid& g = a.g;
