@@ -24,7 +24,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 __all__ = [
-    "BtError", "Options", "Graph", "Gpu", "Info", "Layout", "Snapshot", "Aggregate", "Measurement",
+    "BtError", "Options", "Graph", "Gpu", "Batch", "Info", "Layout", "Snapshot", "Aggregate", "Measurement",
     "squared_integral", "library", "library_path", "build", "COLOR_BY_DENSITY", "COLOR_BY_EDGE_ID", "SIZE",
 ]
 
@@ -101,6 +101,18 @@ SIGNATURES = {
     "bt_distortion": ([_vp, ctypes.c_uint32, _f64p, _f64p], ctypes.c_int32),
     "bt_stage_times": ([_vp, ctypes.POINTER(ctypes.c_char_p), _f32p, ctypes.c_uint32, _u32p], ctypes.c_int32),
     "bt_density_noalloc": ([_vp, _vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_float, _vp], ctypes.c_int32),
+    "bt_batch_create": ([ctypes.c_int32, ctypes.POINTER(_vp)], ctypes.c_int32),
+    "bt_batch_destroy": ([_vp], None),
+    "bt_batch_last_error": ([_vp], ctypes.c_char_p),
+    "bt_batch_add": ([_vp, ctypes.POINTER(_Options), _f32p, ctypes.c_uint32, _u32p, ctypes.c_uint32, _u32p, _u32p],
+                     ctypes.c_int32),
+    "bt_batch_remove": ([_vp, ctypes.c_uint32], ctypes.c_int32),
+    "bt_batch_iterate": ([_vp, ctypes.c_uint32], ctypes.c_int32),
+    "bt_batch_iterate_async": ([_vp, ctypes.c_uint32], ctypes.c_int32),
+    "bt_batch_synchronize": ([_vp], ctypes.c_int32),
+    "bt_batch_iterate_timed": ([_vp, ctypes.c_uint32, _f32p], ctypes.c_int32),
+    "bt_batch_slot_count": ([_vp, _u32p, _u32p], ctypes.c_int32),
+    "bt_batch_slot": ([_vp, ctypes.c_uint32], _vp),
     "bt_graph_parse": ([ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(_vp)], ctypes.c_int32),
     "bt_graph_load": ([ctypes.c_char_p, ctypes.POINTER(_vp)], ctypes.c_int32),
     "bt_graph_free": ([_vp], None),
@@ -413,6 +425,86 @@ class Gpu:
 
     def distortion_snapshot(self, layout: "Layout") -> "Snapshot":
         return layout.decode(self.read_records())
+
+
+class _SlotView(Gpu):
+    """Read-only view of a batch slot's context (owned by the batch)."""
+
+    def __init__(self, handle, options: Options):
+        self.options = options
+        self._h = handle
+
+    def close(self) -> None:  # the batch owns the context
+        self._h = None
+
+
+class Batch:
+    """Many independent graphs advanced together by persistent launches over
+    a graph x tile work queue (bt_batch_*). Each slot keeps its own options;
+    its results equal a single-graph :class:`Gpu` run bit for bit."""
+
+    def __init__(self, device: int = 0):
+        h = _vp()
+        _check(library().bt_batch_create(device, ctypes.byref(h)))
+        self._h = h
+        self._options: dict[int, Options] = {}
+
+    def close(self) -> None:
+        h = getattr(self, "_h", None)
+        if h and _lib is not None:
+            _lib.bt_batch_destroy(h)
+        self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def _ck(self, status: int) -> None:
+        if status:
+            msg = library().bt_batch_last_error(self._h)
+            raise BtError(status, msg.decode() if msg else "")
+
+    def add(self, options: Options, xy: np.ndarray, starts: np.ndarray) -> tuple[int, int]:
+        """Upload a graph into a free slot; returns (slot, samples)."""
+        xy = np.ascontiguousarray(xy, np.float32)
+        starts = np.ascontiguousarray(starts, np.uint32)
+        o = options._struct()
+        slot = ctypes.c_uint32()
+        n = ctypes.c_uint32()
+        self._ck(library().bt_batch_add(self._h, ctypes.byref(o), _p(xy, _f32p), xy.size // 2, _p(starts, _u32p),
+                                        starts.size, ctypes.byref(slot), ctypes.byref(n)))
+        self._options[slot.value] = options
+        return slot.value, n.value
+
+    def remove(self, slot: int) -> None:
+        self._ck(library().bt_batch_remove(self._h, slot))
+        self._options.pop(slot, None)
+
+    def iterate(self, n: int = 1) -> None:
+        self._ck(library().bt_batch_iterate(self._h, n))
+
+    def iterate_async(self, n: int = 1) -> None:
+        self._ck(library().bt_batch_iterate_async(self._h, n))
+
+    def synchronize(self) -> None:
+        self._ck(library().bt_batch_synchronize(self._h))
+
+    def iterate_timed(self, n: int = 1) -> float:
+        ms = np.zeros(1, np.float32)
+        self._ck(library().bt_batch_iterate_timed(self._h, n, _p(ms, _f32p)))
+        return float(ms[0])
+
+    def active(self) -> int:
+        a = ctypes.c_uint32()
+        c = ctypes.c_uint32()
+        self._ck(library().bt_batch_slot_count(self._h, ctypes.byref(a), ctypes.byref(c)))
+        return a.value
+
+    def slot(self, slot: int) -> Gpu:
+        """The slot's context for readbacks (read_points, read_density, ...)."""
+        h = library().bt_batch_slot(self._h, slot)
+        if not h:
+            raise BtError(3, library().bt_batch_last_error(self._h).decode())
+        return _SlotView(h, self._options[slot])
 
 
 @dataclass

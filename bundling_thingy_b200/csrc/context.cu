@@ -15,11 +15,15 @@
 #include <vector>
 
 #include "bt.h"
+#include "context.h"
 #include "host.h"
 #include "kernels.cuh"
 #include "scan.cuh"
 
 namespace {
+
+using bt::DevBuf;
+using bt::StageRec;
 
 thread_local std::string g_thread_error;
 
@@ -27,66 +31,6 @@ constexpr uint64_t kMiB = 1024ull * 1024ull;
 constexpr uint64_t kDistortionStagingBytes = 4194300;   // resampling.rs:16
 constexpr uint32_t kMaxDimension = 32768;
 constexpr double kWaitSeconds = 60.0;                   // gpu.rs:484-490
-
-struct DevBuf {
-    void* p = nullptr;
-    size_t bytes = 0;
-    template <typename T>
-    T* as() const {
-        return static_cast<T*>(p);
-    }
-};
-
-struct StageRec {
-    const char* name;
-    cudaEvent_t start, stop;
-};
-
-}  // namespace
-
-struct bt_graph {
-    bt::HostGraph g;
-};
-
-struct bt_ctx {
-    bt_options opt{};
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    cudaEvent_t done = nullptr;
-    cudaEvent_t t0 = nullptr, t1 = nullptr;
-    std::string err;
-
-    bt::Map map{};
-    bt::Grid grid{};
-    bool has_grid = false, accumulate = false;
-    float rsx = 0.f, rsy = 0.f;
-    uint64_t grid_bytes_ref = 0, staging_ref = 0;
-    size_t cells = 0, texels = 0;
-
-    DevBuf cp, starts, packed, offsets, scan64, edges, paths, totals, status;
-    DevBuf edge_ids, segments, tmp_xy, tmp_tag, tmp_cell, neighbors, baseline, current;
-    DevBuf sorted_rec[2], sorted_tag[2];
-    DevBuf hist, cellsum, cell_start, cell_prefix, table_scratch;
-    DevBuf counts, himg, vimg, norm, peak;
-    DevBuf records, integrals;
-    unsigned long long* h_totals = nullptr;   // pinned
-    uint32_t* h_status = nullptr;             // pinned
-    size_t device_bytes = 0;
-
-    bool uploaded = false;
-    uint32_t samples = 0, n_paths = 0, drawn = 0, capacity = 0;
-    uint64_t reserved_bytes = 0;
-    uint32_t iterations = 0, density_passes = 0;
-    int cur = 0;
-
-    cudaGraphExec_t graphs[2] = {nullptr, nullptr};
-
-    std::vector<StageRec> stage_log;
-    std::vector<StageRec> stage_pool;
-    size_t stage_used = 0;
-};
-
-namespace {
 
 bt_status fail(bt_ctx* c, bt_status code, const std::string& msg) {
     if (c) c->err = msg;
@@ -321,6 +265,7 @@ namespace bt {
 // Shared with the allocation-free density entry point (density_noalloc.cu).
 bool make_blur_taps(double sigma, Taps* taps) { return blur_taps(sigma, taps); }
 void set_thread_error(const char* message) { g_thread_error = message; }
+double sigma_for_pass(const bt_options& options, uint32_t pass) { return ::sigma_for_pass(options, pass); }
 }  // namespace bt
 
 extern "C" {

@@ -1,0 +1,206 @@
+// grid_dev.cuh — per-sample bodies of the neighbour-mean and scatter kernels,
+// shared by the single-graph kernels (grid.cu) and the batched persistent
+// kernels (batch.cu). See grid.cu for the semantics and the layout.
+#pragma once
+
+#include "kernels.cuh"
+
+namespace bt {
+namespace dev {
+
+// Search-cell index bounds t / s, by the reciprocal: the bounds are
+// conservative by the margin, which exceeds this rounding many times over.
+__device__ __forceinline__ int floor_cell(float t, float inv_s) { return static_cast<int>(floorf(t * inv_s)); }
+__device__ __forceinline__ int ceil_cell(float t, float inv_s) { return static_cast<int>(ceilf(t * inv_s)); }
+
+// Approximate square root (one MUFU op); callers widen its result by a
+// relative 1e-6 plus the margin, far above its error.
+__device__ __forceinline__ float sqrt_approx(float x) {
+    float r;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+struct Acc {
+    unsigned long long sx, sy;
+    uint32_t count;
+};
+
+// Exact test of every sample in slots [b, e) (neighbor_mean.wgsl:193-198).
+__device__ __forceinline__ void scan_range(const uint4* __restrict__ rec, uint32_t b, uint32_t e, float2 neg_p,
+                                           float2 ts, float r2, Acc& acc) {
+#pragma unroll 4
+    for (uint32_t j = b; j < e; ++j) {
+        const uint4 q = __ldg(rec + j);
+        const float2 d = __fadd2_rn(make_float2(__uint_as_float(q.x), __uint_as_float(q.y)), neg_p);
+        const float2 t = __fmul2_rn(d, ts);
+        const float2 t2 = __fmul2_rn(t, t);
+        const float d2 = t2.x + t2.y;
+        if (d2 <= r2) {
+            acc.sx += q.z;
+            acc.sy += q.w;
+            acc.count += 1u;
+        }
+    }
+}
+
+// Neighbour mean of the sample in slot i (i >= a.n: an idle lane). Every
+// lane of the warp must call it: the next-grid counts are warp-aggregated.
+__device__ __forceinline__ void mean_sample(const MeanArgs& a, uint32_t i) {
+    const bool valid = i < a.n;
+    const Grid& g = a.g;
+    const uint4 me = valid ? a.rec[i] : make_uint4(0u, 0u, 0u, 0u);
+    const float2 p = make_float2(__uint_as_float(me.x), __uint_as_float(me.y));
+    const uint32_t tag = valid ? a.tag[i] : 0u;
+    float2 np = p;
+    uint32_t count = 0;
+    if (tag & kMovableBit) {
+        const float tx = texel_of(p.x, g.map.wm1), ty = texel_of(p.y, g.map.hm1);
+        // Reach box in grid cells (neighbor_mean.wgsl:180-185), in search cells.
+        const uint32_t cx0 = grid_of(tx - g.reachx, g.rf, g.gw), cx1 = grid_of(tx + g.reachx, g.rf, g.gw);
+        const uint32_t cy0 = grid_of(ty - g.reachy, g.rf, g.gh), cy1 = grid_of(ty + g.reachy, g.rf, g.gh);
+        const int fx_min = static_cast<int>(cx0 * g.k), fx_max = static_cast<int>(cx1 * g.k + g.k - 1u);
+        const int fy_min = static_cast<int>(cy0 * g.k), fy_max = static_cast<int>(cy1 * g.k + g.k - 1u);
+        // Candidate circle r + m; certain circle r - m (texels).
+        const float R = g.rf + g.margin;
+        const float Rin = g.rf - g.margin;
+        const int fy_lo = max(fy_min, floor_cell(ty - R, g.inv_s));
+        const int fy_hi = min(fy_max, floor_cell(ty + R, g.inv_s));
+        const bool interior = a.mode == kSearchInterior;
+        const int fw = static_cast<int>(g.fw), fh = static_cast<int>(g.fh);
+        const float2 neg_p = make_float2(-p.x, -p.y);
+        const float2 ts = make_float2(g.tsx, g.tsy);
+        Acc acc{0ull, 0ull, 0u};
+        for (int fy = fy_lo; fy <= fy_hi; ++fy) {
+            const float ylo = static_cast<float>(fy) * g.s;
+            const float yhi = ylo + g.s;
+            const float near = fmaxf(fmaxf(ylo - ty, ty - yhi), 0.0f);
+            const float dn = fmaxf(near - g.margin, 0.0f);
+            if (dn > R) continue;
+            // f32 rounding of R^2 - dn^2 is below 5e-7 R^2; widen by that.
+            const float hout = sqrt_approx(fmaxf(R * R - dn * dn + 5e-7f * R * R, 0.0f)) * 1.000001f + g.margin;
+            const int bx0 = max(fx_min, floor_cell(tx - hout, g.inv_s));
+            const int bx1 = min(fx_max, floor_cell(tx + hout, g.inv_s));
+            if (bx0 > bx1) continue;
+            const uint32_t row = static_cast<uint32_t>(fy) * g.fw;
+            const uint32_t s0 = a.cell_start[row + bx0];
+            const uint32_t s3 = a.cell_start[row + bx1 + 1];
+            int ix0 = 1, ix1 = 0;
+            if (interior && fy > 0 && fy < fh - 1) {
+                // Cells of this row whose every sample passes the f32 test:
+                // the farthest point of the row band, widened by the margin.
+                const float far = fmaxf(fabsf(ylo - ty), fabsf(yhi - ty)) + g.margin;
+                if (far < Rin) {
+                    const float h2 = Rin * Rin - far * far - 5e-7f * Rin * Rin;
+                    const float hin = sqrt_approx(fmaxf(h2, 0.0f)) * 0.999999f - g.margin;
+                    if (hin > 0.0f) {
+                        ix0 = max(ceil_cell(tx - hin, g.inv_s), max(bx0, 1));
+                        ix1 = min(floor_cell(tx + hin, g.inv_s) - 1, min(bx1, fw - 2));
+                    }
+                }
+            }
+            if (ix0 <= ix1) {
+                const uint32_t s1 = a.cell_start[row + ix0];
+                const uint32_t s2 = a.cell_start[row + ix1 + 1];
+                const LL2 lo = a.cell_prefix[row + ix0], hi = a.cell_prefix[row + ix1 + 1];
+                acc.sx += static_cast<unsigned long long>(hi.x - lo.x);
+                acc.sy += static_cast<unsigned long long>(hi.y - lo.y);
+                acc.count += s2 - s1;
+                scan_range(a.rec, s0, s1, neg_p, ts, g.r2, acc);
+                scan_range(a.rec, s2, s3, neg_p, ts, g.r2, acc);
+            } else {
+                scan_range(a.rec, s0, s3, neg_p, ts, g.r2, acc);
+            }
+        }
+        count = acc.count;
+        // Biased sums: sum (Q(q) + B) - n (Q(p) + B) = sum Q(q) - n Q(p).
+        const long long dx = static_cast<long long>(acc.sx - static_cast<unsigned long long>(count) * me.z);
+        const long long dy = static_cast<long long>(acc.sy - static_cast<unsigned long long>(count) * me.w);
+        const double den = static_cast<double>(count) * 1073741824.0;
+        np.x = p.x + static_cast<float>(static_cast<double>(dx) / den);
+        np.y = p.y + static_cast<float>(static_cast<double>(dy) / den);
+    }
+    // The next grid: search cell, population and biased position sum. Lanes
+    // of a warp that land in one cell (neighbours in slot order mostly do)
+    // add their counts and sums once.
+    const uint32_t c = valid ? search_cell(np, g) : 0xFFFFFFFFu;
+    const unsigned peers = __match_any_sync(0xFFFFFFFFu, c);
+    if (!valid) return;
+    const uint32_t qx = biased_fixed(np.x), qy = biased_fixed(np.y);
+    // Group sums in 16-bit halves so each 32-bit reduction cannot overflow.
+    const uint32_t xl = __reduce_add_sync(peers, qx & 0xFFFFu), xh = __reduce_add_sync(peers, qx >> 16);
+    const uint32_t yl = __reduce_add_sync(peers, qy & 0xFFFFu), yh = __reduce_add_sync(peers, qy >> 16);
+    if ((threadIdx.x & 31) == __ffs(peers) - 1) {
+        atomicAdd(&a.hist[c], static_cast<uint32_t>(__popc(peers)));
+        atomicAdd(reinterpret_cast<unsigned long long*>(&a.cellsum[c].x),
+                  (static_cast<unsigned long long>(xh) << 16) + xl);
+        atomicAdd(reinterpret_cast<unsigned long long*>(&a.cellsum[c].y),
+                  (static_cast<unsigned long long>(yh) << 16) + yl);
+    }
+    a.out_xy[i] = np;
+    a.out_tag[i] = tag;
+    a.out_cell[i] = c;
+    if (a.counts) {
+        uint32_t d;
+        if (splat_index(np.x, np.y, g.map, &d)) atomicAdd(&a.counts[d], 1u);
+    }
+    if (a.neighbors) a.neighbors[i] = count;
+}
+
+// Slot of sample i in the next order: start of its search cell plus a rank
+// taken by counting the population down (order within a cell is free: the
+// mean's exact sum does not depend on it). Every lane of the warp calls it.
+__device__ __forceinline__ void scatter_sample(const ScatterArgs& a, uint32_t i) {
+    const bool valid = i < a.n;
+    const uint32_t c = valid ? a.cell[i] : 0xFFFFFFFFu;
+    // Lanes of one warp that share a cell (neighbours in slot order mostly do)
+    // take one reservation and consecutive slots, so their writes coalesce.
+    const unsigned peers = __match_any_sync(0xFFFFFFFFu, c);
+    if (!valid) return;
+    // Cell ids and populations are consistent by construction; a failed
+    // upload can leave stale entries, which are skipped and flagged.
+    if (c >= a.cells) {
+        atomicOr(a.status, 8u);
+        return;
+    }
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(peers) - 1;
+    const uint32_t group = __popc(peers);
+    const uint32_t rank = __popc(peers & ((1u << lane) - 1u));
+    uint32_t top = 0;
+    if (lane == leader) top = atomicSub(&a.hist[c], group);
+    top = __shfl_sync(peers, top, leader);
+    const uint32_t slot = a.cell_start[c] + (top - group) + rank;
+    if (top < group || slot >= a.n) {
+        atomicOr(a.status, 8u);
+        return;
+    }
+    const float2 p = a.xy[i];
+    a.out_rec[slot] = make_uint4(__float_as_uint(p.x), __float_as_uint(p.y), biased_fixed(p.x), biased_fixed(p.y));
+    a.out_tag[slot] = a.tag[i];
+}
+
+// Cell-table scan input: a cell's population and position sums; the sums are
+// cleared after their last read so the next iteration accumulates from zero.
+struct CellAccSource {
+    const uint32_t* hist;
+    LL2* cellsum;
+    __device__ __forceinline__ LL3 read(size_t j) const {
+        const LL2 s = cellsum[j];
+        return LL3{static_cast<long long>(hist[j]), s.x, s.y};
+    }
+    __device__ __forceinline__ void consume(size_t j) const { cellsum[j] = LL2{0, 0}; }
+};
+
+// Cell-table scan output: first slot and prefix sums of each search cell.
+struct CellTableSink {
+    uint32_t* cell_start;
+    LL2* cell_prefix;
+    __device__ __forceinline__ void store(size_t j, LL3 v) const {
+        cell_start[j] = static_cast<uint32_t>(v.c);
+        cell_prefix[j] = LL2{v.x, v.y};
+    }
+};
+
+}  // namespace dev
+}  // namespace bt

@@ -157,39 +157,43 @@ __device__ __forceinline__ T block_exclusive(T v, T* warp_sums, T* total) {
     return prefix;
 }
 
+// Shared memory of one tile pass (padded to avoid bank conflicts).
+template <typename T>
+struct ScanShared {
+    T tile[scan_tile<T>() + scan_tile<T>() / 32];
+    T warp_sums[kScanBlock / 32 + 1];
+};
+
+// Sum of in[base .. min(base + tile, n)) over the block (all threads get it).
 template <typename T, typename Source>
-__global__ void __launch_bounds__(kScanBlock) scan_reduce_kernel(Source in, size_t n, T* sums) {
-    __shared__ T warp_sums[kScanBlock / 32 + 1];
+__device__ __forceinline__ T tile_reduce(const Source& in, size_t base, size_t n, ScanShared<T>& sh) {
     constexpr int kItems = scan_items<T>();
-    const size_t base = static_cast<size_t>(blockIdx.x) * scan_tile<T>();
     T acc = zero<T>();
 #pragma unroll
     for (int i = 0; i < kItems; ++i) {
         size_t j = base + static_cast<size_t>(i) * kScanBlock + threadIdx.x;
         if (j < n) acc += in.read(j);
     }
-    acc = block_sum(acc, warp_sums);
-    if (threadIdx.x == 0) sums[blockIdx.x] = acc;
+    return block_sum(acc, sh.warp_sums);
 }
 
-// out[j] = offsets[block] + sum(in[tile start .. j)); out[n] = total.
+// out[j] = offset + sum(in[base .. j)) for the tile at base; the tile that
+// reaches n also stores the total at n. Synchronises internally.
 template <typename T, typename Source, typename Sink>
-__global__ void __launch_bounds__(kScanBlock) scan_apply_kernel(Source in, size_t n, const T* offsets, Sink out) {
+__device__ __forceinline__ void tile_apply(const Source& in, const Sink& out, size_t base, size_t n, T offset,
+                                           ScanShared<T>& sh) {
     constexpr int kItems = scan_items<T>();
     constexpr int kTile = kScanBlock * kItems;
-    __shared__ T tile[kTile + kTile / 32];
-    __shared__ T warp_sums[kScanBlock / 32 + 1];
-    const size_t base = static_cast<size_t>(blockIdx.x) * kTile;
     auto pad = [](int i) { return i + (i >> 5); };
 #pragma unroll
     for (int i = 0; i < kItems; ++i) {
         int t = i * kScanBlock + threadIdx.x;
         size_t j = base + t;
         if (j < n) {
-            tile[pad(t)] = in.read(j);
+            sh.tile[pad(t)] = in.read(j);
             in.consume(j);
         } else {
-            tile[pad(t)] = zero<T>();
+            sh.tile[pad(t)] = zero<T>();
         }
     }
     __syncthreads();
@@ -197,16 +201,15 @@ __global__ void __launch_bounds__(kScanBlock) scan_apply_kernel(Source in, size_
     T sum = zero<T>();
 #pragma unroll
     for (int i = 0; i < kItems; ++i) {
-        local[i] = tile[pad(threadIdx.x * kItems + i)];
+        local[i] = sh.tile[pad(threadIdx.x * kItems + i)];
         sum += local[i];
     }
     T block_total;
-    T prefix = block_exclusive(sum, warp_sums, &block_total);
-    const T offset = offsets ? offsets[blockIdx.x] : zero<T>();
+    T prefix = block_exclusive(sum, sh.warp_sums, &block_total);
     prefix += offset;
 #pragma unroll
     for (int i = 0; i < kItems; ++i) {
-        tile[pad(threadIdx.x * kItems + i)] = prefix;
+        sh.tile[pad(threadIdx.x * kItems + i)] = prefix;
         prefix += local[i];
     }
     __syncthreads();
@@ -214,9 +217,25 @@ __global__ void __launch_bounds__(kScanBlock) scan_apply_kernel(Source in, size_
     for (int i = 0; i < kItems; ++i) {
         int t = i * kScanBlock + threadIdx.x;
         size_t j = base + t;
-        if (j < n) out.store(j, tile[pad(t)]);
+        if (j < n) out.store(j, sh.tile[pad(t)]);
     }
     if (threadIdx.x == 0 && base + kTile >= n) out.store(n, offset + block_total);
+    __syncthreads();
+}
+
+template <typename T, typename Source>
+__global__ void __launch_bounds__(kScanBlock) scan_reduce_kernel(Source in, size_t n, T* sums) {
+    __shared__ ScanShared<T> sh;
+    const T total = tile_reduce<T>(in, static_cast<size_t>(blockIdx.x) * scan_tile<T>(), n, sh);
+    if (threadIdx.x == 0) sums[blockIdx.x] = total;
+}
+
+// out[j] = offsets[block] + sum(in[tile start .. j)); out[n] = total.
+template <typename T, typename Source, typename Sink>
+__global__ void __launch_bounds__(kScanBlock) scan_apply_kernel(Source in, size_t n, const T* offsets, Sink out) {
+    __shared__ ScanShared<T> sh;
+    const T offset = offsets ? offsets[blockIdx.x] : zero<T>();
+    tile_apply<T>(in, out, static_cast<size_t>(blockIdx.x) * scan_tile<T>(), n, offset, sh);
 }
 
 // Each level keeps its block sums and their scan (blocks + 1 entries each).

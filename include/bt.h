@@ -168,6 +168,36 @@ bt_status bt_distortion(bt_ctx* ctx, uint32_t size, double* distortion, double* 
  * entries; returns the number of stages in *count. */
 bt_status bt_stage_times(bt_ctx* ctx, const char** names, float* ms, uint32_t capacity, uint32_t* count);
 
+/* ---- Batches: many independent graphs per launch ----
+ *
+ * Beyond the reference (which bundles one graph at a time, src/main.rs:113-126):
+ * each graph occupies a slot with its own options (map size, radius, sigma,
+ * spacing); bt_batch_iterate advances every active slot by n iterations of
+ * Gpu::iterate with one set of persistent launches over a graph x tile work
+ * queue, captured in a CUDA graph. A slot's results equal a bt_ctx run of the
+ * same graph bit for bit, whatever else is in the batch. */
+typedef struct bt_batch bt_batch;
+
+bt_status bt_batch_create(int32_t device, bt_batch** out);
+void bt_batch_destroy(bt_batch* batch);
+const char* bt_batch_last_error(const bt_batch* batch);
+/* Uploads one graph (bt_create + bt_upload with `options`; neighbor_radius
+ * must be set) into a free slot; returns its slot index and sample count. */
+bt_status bt_batch_add(bt_batch* batch, const bt_options* options, const float* xy, uint32_t n_points,
+                       const uint32_t* starts, uint32_t n_starts, uint32_t* slot, uint32_t* samples);
+/* Releases a slot (its index may be reused by a later add). */
+bt_status bt_batch_remove(bt_batch* batch, uint32_t slot);
+/* n iterations of every active slot; waits for the device. */
+bt_status bt_batch_iterate(bt_batch* batch, uint32_t n);
+bt_status bt_batch_iterate_async(bt_batch* batch, uint32_t n);
+bt_status bt_batch_synchronize(bt_batch* batch);
+/* bt_batch_iterate with the device milliseconds of the n iterations. */
+bt_status bt_batch_iterate_timed(bt_batch* batch, uint32_t n, float* device_ms);
+bt_status bt_batch_slot_count(bt_batch* batch, uint32_t* active, uint32_t* capacity);
+/* The context of a slot, for the bt_read_* and bt_get_info calls; owned by
+ * the batch (do not destroy or iterate it). Waits for the batch's work. */
+bt_ctx* bt_batch_slot(bt_batch* batch, uint32_t slot);
+
 /* ---- Density blur without allocation ---- */
 
 /* Largest width*height accepted by bt_density_noalloc: its static device

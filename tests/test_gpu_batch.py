@@ -1,0 +1,126 @@
+"""Batches: every slot's results equal a standalone run of the same graph.
+
+The batch advances all of its graphs with persistent launches over a
+graph x tile work queue; a graph's results must not depend on what else is
+in the batch (alone vs in the mix), bit for bit.
+"""
+import numpy as np
+import pytest
+
+import bundling_thingy_b200 as bt
+from bundling_thingy_b200 import synthetic
+
+from conftest import oracle_config
+
+pytestmark = pytest.mark.gpu
+
+
+def workload_options(w, **kw):
+    o = bt.Options(width=w.width, height=w.height, neighbor_radius=w.radius, sample_spacing=w.spacing,
+                   blur_sigma=w.sigma, blur_shrink=w.shrink)
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+def mixed_jobs():
+    small, mid = synthetic.small(), synthetic.mid()
+    small2 = synthetic.small(seed_offset=11)
+    return [
+        (small, workload_options(small)),                                   # shrinking sigma
+        (mid, workload_options(mid)),
+        (small2, bt.Options(neighbor_radius=4)),                            # reference settings, 1600^2
+        (small2, workload_options(small2, color_by=bt.COLOR_BY_EDGE_ID)),   # no density passes
+        (small, workload_options(small, width=512, height=512, neighbor_radius=1, blur_sigma=3.0,
+                                 blur_shrink=1.0, search_mode=1)),
+    ]
+
+
+def standalone(w, o, iterations):
+    g = bt.Gpu(o)
+    g.upload((w.xy, w.starts))
+    if iterations:
+        g.iterate(iterations)
+    xy, ids = g.read_points()
+    dens = g.read_density() if o.color_by == bt.COLOR_BY_DENSITY else None
+    g.close()
+    return xy, ids, dens
+
+
+def check_slot(batch, slot, expected):
+    view = batch.slot(slot)
+    xy, ids = view.read_points()
+    np.testing.assert_array_equal(ids, expected[1])
+    np.testing.assert_array_equal(xy, expected[0])
+    if expected[2] is not None:
+        np.testing.assert_array_equal(view.read_density(), expected[2])
+
+
+def test_mixed_batch_matches_standalone_runs():
+    jobs = mixed_jobs()
+    batch = bt.Batch()
+    slots = [batch.add(o, w.xy, w.starts)[0] for w, o in jobs]
+    assert batch.active() == len(jobs)
+    batch.iterate(3)
+    for (w, o), slot in zip(jobs, slots):
+        check_slot(batch, slot, standalone(w, o, 3))
+    batch.iterate(2)
+    for (w, o), slot in zip(jobs, slots):
+        check_slot(batch, slot, standalone(w, o, 5))
+    info = batch.slot(slots[0]).info()
+    assert info.iterations == 5
+
+
+def test_first_slot_matches_oracle(oracle):
+    w = synthetic.small()
+    o = workload_options(w)
+    batch = bt.Batch()
+    slot, n = batch.add(o, w.xy, w.starts)
+    batch.add(*(lambda m: (workload_options(m), m.xy, m.starts))(synthetic.mid()))
+    batch.iterate(4)
+    ora = oracle.Pipeline(oracle_config(oracle, o))
+    assert ora.upload(w.xy, w.starts) == n
+    ora.iterate(4)
+    xy, ids = batch.slot(slot).read_points()
+    oxy, oids = ora.points()
+    np.testing.assert_array_equal(ids, oids)
+    np.testing.assert_array_equal(xy, oxy)
+    np.testing.assert_array_equal(batch.slot(slot).read_density(), ora.normalized())
+
+
+def test_slots_join_and_leave_between_iterations():
+    jobs = mixed_jobs()
+    batch = bt.Batch()
+    a = batch.add(jobs[0][1], jobs[0][0].xy, jobs[0][0].starts)[0]
+    b = batch.add(jobs[1][1], jobs[1][0].xy, jobs[1][0].starts)[0]
+    batch.iterate(1)                       # a, b at parity 1
+    c = batch.add(jobs[2][1], jobs[2][0].xy, jobs[2][0].starts)[0]
+    batch.iterate(2)                       # a, b: 3 iterations; c: 2
+    batch.remove(a)
+    d = batch.add(jobs[4][1], jobs[4][0].xy, jobs[4][0].starts)[0]
+    assert d == a                          # the freed slot is reused
+    batch.iterate(1)                       # b: 4, c: 3, d: 1
+    check_slot(batch, b, standalone(*jobs[1], 4))
+    check_slot(batch, c, standalone(*jobs[2], 3))
+    check_slot(batch, d, standalone(*jobs[4], 1))
+
+
+def test_long_shrinking_sigma_run_extends_taps():
+    w = synthetic.small()
+    o = workload_options(w)
+    batch = bt.Batch()
+    slot = batch.add(o, w.xy, w.starts)[0]
+    batch.iterate(70)                      # beyond the precomputed taps horizon
+    check_slot(batch, slot, standalone(w, o, 70))
+
+
+def test_batch_errors():
+    batch = bt.Batch()
+    w = synthetic.small()
+    with pytest.raises(bt.BtError) as e:
+        batch.add(bt.Options(width=256, height=256), w.xy, w.starts)
+    assert e.value.status == 8
+    with pytest.raises(bt.BtError):
+        batch.remove(3)
+    batch.iterate(2)                       # an empty batch is a no-op
+    assert batch.active() == 0
