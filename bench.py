@@ -51,6 +51,16 @@ def parse_args():
     p.add_argument("--e2e-jobs", type=int, default=3)
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU work of the baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--workload", choices=["large", "batched", "served"], default="large")
+    p.add_argument("--graphs", type=int, default=256, help="batched workload: number of graphs")
+    p.add_argument("--batch-iterations", type=int, default=10)
+    p.add_argument("--requests", type=int, default=1000, help="served workload: requests per rank")
+    p.add_argument("--rate", type=float, default=200.0, help="served workload: mean arrivals per second")
+    p.add_argument("--capacity-requests", type=int, default=300,
+                   help="served workload: requests of the all-at-once capacity run (0 = skip)")
+    p.add_argument("--max-active", type=int, default=32)
+    p.add_argument("--max-step", type=int, default=1)
+    p.add_argument("--budget-gb", type=float, default=120.0)
     return p.parse_args()
 
 
@@ -361,12 +371,299 @@ def run_ours(args, ranks: Ranks):
         print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------- batched
+def run_batched(args, ranks: Ranks):
+    """256 independent graphs (edges log-uniform 200-20,000, grids 256/512/1024),
+    10 iterations each: one batch (persistent launches over graph x tile,
+    CUDA-graph iteration) against the plain per-graph loop. Graphs are
+    sharded across ranks by index (no collective)."""
+    import torch
+
+    import bundling_thingy_b200 as bt
+    from bundling_thingy_b200 import synthetic
+
+    device = ranks.local
+    iters = args.batch_iterations
+    jobs = synthetic.batched_jobs(args.graphs, iterations=iters)[ranks.rank::ranks.world]
+
+    def key(j):
+        return (j.width, j.radius)
+
+    def options(j):
+        return bt.Options(width=j.width, height=j.height, neighbor_radius=j.radius, sample_spacing=j.spacing,
+                          blur_sigma=j.sigma, device=device)
+
+    # Autotune the search-cell size once per (grid, radius) class.
+    t0 = time.perf_counter()
+    firsts = {}
+    for j in jobs:
+        firsts.setdefault(key(j), j)
+    tuned = {}
+    for k, j in firsts.items():
+        o, ms = bt.autotune(options(j), j.xy, j.starts, 3)
+        tuned[k] = {"fine_cells": o.fine_cells, "ms_3_iterations": ms}
+    autotune_s = time.perf_counter() - t0
+
+    def tuned_options(j):
+        o = options(j)
+        o.fine_cells = tuned[key(j)]["fine_cells"]
+        return o
+
+    # Plain per-graph loop: one context per class, reused (Gpu::upload
+    # releases the previous graph), upload + 10 x iterate + readback.
+    # Results are read into one reused pinned host buffer in both arms.
+    host = {"buf": None}
+
+    def read(g):
+        n = 12 * g.info().samples
+        if host["buf"] is None or host["buf"].nbytes < n:
+            host["buf"] = torch.empty(max(n, 96 << 20), dtype=torch.uint8, pin_memory=True).numpy()
+        return g.read_records(host["buf"])
+
+    ctxs = {k: bt.Gpu(tuned_options(j)) for k, j in firsts.items()}
+    for k, j in firsts.items():            # warm-up
+        ctxs[k].upload((j.xy, j.starts))
+        ctxs[k].iterate(1)
+        read(ctxs[k])
+    ranks.barrier()
+    plain_results = {}
+    t0 = time.perf_counter()
+    t_iter = 0.0
+    for idx, j in enumerate(jobs):
+        g = ctxs[key(j)]
+        g.upload((j.xy, j.starts))
+        ti = time.perf_counter()
+        g.iterate(iters)
+        t_iter += time.perf_counter() - ti
+        rec = read(g)
+        if idx < 4:
+            plain_results[idx] = rec.copy()
+    plain_s = time.perf_counter() - t0
+    for g in ctxs.values():
+        g.close()
+
+    # Warm the batch kernels once (module load, first graph capture).
+    warm = bt.Batch(device)
+    warm.add_many([(tuned_options(j), j.xy, j.starts) for j in firsts.values()])
+    warm.iterate(1)
+    warm.close()
+
+    # Batched: upload every graph concurrently, one batched call for all
+    # iterations, readback.
+    ranks.barrier()
+    t0 = time.perf_counter()
+    batch = bt.Batch(device)
+    slots = [s for s, _ in batch.add_many([(tuned_options(j), j.xy, j.starts) for j in jobs])]
+    t_add = time.perf_counter() - t0
+    ti = time.perf_counter()
+    batch.iterate(iters)
+    batch_iter_s = time.perf_counter() - ti
+    outs = {}
+    for idx, s in enumerate(slots):
+        rec = read(batch.slot(s))
+        if idx < 4:
+            outs[idx] = rec.copy()
+    batch_s = time.perf_counter() - t0
+    exact = all(np.array_equal(outs[i], plain_results[i]) for i in plain_results)
+    samples = sum(batch.slot(s).info().samples for s in slots)
+    # Device time of the batched iterations alone (CUDA events).
+    dev_ms = batch.iterate_timed(iters)
+    batch.close()
+
+    graphs = ranks.sum(len(jobs))
+    batch_gps = graphs / ranks.max(batch_s)
+    plain_gps = graphs / ranks.max(plain_s)
+    line = {
+        "metric": "batched graphs/s (256 graphs, 10 iterations each)", "value": batch_gps, "unit": "graphs/s",
+        "n_gpus": ranks.world, "higher_is_better": True, "scaling": "weak", "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "batched: 256 graphs, edges log-uniform 200-20k, grids 256/512/1024, 10 iterations",
+                   "samples": int(ranks.sum(samples)), "parallelism": f"graphs sharded x{ranks.world}"},
+        "plain_graphs_per_s": plain_gps, "speedup_vs_plain": batch_gps / plain_gps,
+        "batch_seconds": {"add_uploads": t_add, "iterations": batch_iter_s, "total": batch_s},
+        "plain_seconds": {"iterations": t_iter, "total": plain_s},
+        "batched_points_iter_per_s_device": ranks.sum(samples * iters) / (ranks.max(dev_ms) / 1e3),
+        "iteration_speedup_vs_plain": t_iter / batch_iter_s,
+        "autotune": {"seconds": autotune_s, "classes": {f"{k[0]}px r{k[1]}": v for k, v in tuned.items()}},
+        "bit_exact_vs_plain": exact,
+    }
+    if ranks.rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def run_served(args, ranks: Ranks):
+    """Poisson-arriving requests (mean 200/s; edges log-uniform 500-50,000;
+    grids 512/1024/2048; 10 iterations each; 120 GB admission budget): the
+    continuous-batching server against the plain per-request loop, both
+    replaying the same arrival schedule and reading every result back to
+    pinned host memory. Each rank serves its own arrival stream (weak
+    scaling, no collective)."""
+    import torch
+
+    import bundling_thingy_b200 as bt
+    from bundling_thingy_b200 import synthetic
+
+    device = ranks.local
+    iters = args.batch_iterations
+    arrivals, jobs = synthetic.served_jobs(args.requests, rate=args.rate, iterations=iters,
+                                           seed=synthetic.SEED_BASE + 4 + 7919 * ranks.rank)
+    n = len(jobs)
+
+    def key(j):
+        return (j.width, j.radius)
+
+    def options(j):
+        return bt.Options(width=j.width, height=j.height, neighbor_radius=j.radius, sample_spacing=j.spacing,
+                          blur_sigma=j.sigma, device=device)
+
+    firsts = {}   # (grid, radius) class -> index of its first request
+    for i, j in enumerate(jobs):
+        firsts.setdefault(key(j), i)
+    tuned = {}
+    for k, i in firsts.items():
+        o, _ = bt.autotune(options(jobs[i]), jobs[i].xy, jobs[i].starts, 3)
+        tuned[k] = o.fine_cells
+    opts = []
+    for j in jobs:
+        o = options(j)
+        o.fine_cells = tuned[key(j)]
+        opts.append(o)
+
+    host = {"buf": None}
+
+    def pinned(nbytes):
+        if host["buf"] is None or host["buf"].nbytes < nbytes:
+            host["buf"] = torch.empty(max(nbytes, 128 << 20), dtype=torch.uint8, pin_memory=True).numpy()
+        return host["buf"]
+
+    keep = 4   # results compared between the arms
+
+    def plain_run(sched):
+        """Plain per-request loop: one reused context per (grid, radius)
+        class; upload, 10 iterations, read back, in arrival order."""
+        ctxs = {}
+        for k, i in firsts.items():
+            j = jobs[i]
+            g = bt.Gpu(opts[i])
+            g.upload((j.xy, j.starts))
+            g.iterate(1)
+            g.read_records(pinned(12 * g.info().samples))
+            ctxs[k] = g
+        lat, kept, samples = [], {}, 0
+        base = time.perf_counter() + 0.05
+        t_end = base
+        for i, (a, j) in enumerate(zip(sched, jobs[: len(sched)])):
+            target = base + a
+            wait = target - time.perf_counter()
+            if wait > 0:
+                time.sleep(wait)
+            g = ctxs[key(j)]
+            nsamp = g.upload((j.xy, j.starts))
+            g.iterate(iters)
+            rec = g.read_records(pinned(12 * nsamp))
+            t_end = time.perf_counter()
+            lat.append(t_end - target)
+            samples += nsamp
+            if i < keep:
+                kept[i] = rec.copy()
+        for g in ctxs.values():
+            g.close()
+        return lat, t_end - (base + sched[0]), samples, kept
+
+    def served_run(sched):
+        server = bt.Server(device, max_active=args.max_active, budget_bytes=int(args.budget_gb * 1e9),
+                           max_step=args.max_step)
+        # Warm-up: one request per class (kernels, first graph captures, and
+        # one idle context per class, like the plain loop's reused contexts).
+        for i in firsts.values():
+            server.submit(opts[i], jobs[i].xy, jobs[i].starts, 1)
+        for _ in firsts:
+            r = server.next(120.0)
+            server.read_records(r.id, r.samples, pinned(12 * r.samples))
+            server.release(r.id)
+        t0 = time.perf_counter()
+        base = server.clock() + 1.0 + 2e-3 * len(sched)   # after every submission
+        ids = {}
+        for i, (a, j) in enumerate(zip(sched, jobs[: len(sched)])):
+            ids[server.submit(opts[i], j.xy, j.starts, iters, arrival_s=base + a)] = i
+        submit_s = time.perf_counter() - t0
+        late = server.clock() > base
+        lat, kept, samples, t_end = [], {}, 0, base
+        for _ in range(len(sched)):
+            r = server.next(300.0)
+            if r.status != 0:
+                raise RuntimeError(f"request {r.id} failed: {r.message}")
+            rec = server.read_records(r.id, r.samples, pinned(12 * r.samples))
+            t_end = server.clock()
+            lat.append(t_end - r.arrival_s)
+            samples += r.samples
+            if ids[r.id] < keep:
+                kept[ids[r.id]] = rec.copy()
+            server.release(r.id)
+        stats = server.stats()
+        server.close()
+        return lat, t_end - (base + sched[0]), samples, kept, stats, submit_s, late
+
+    def pct(lat):
+        return {"p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
+                "max_ms": float(np.max(lat) * 1e3)}
+
+    ranks.barrier()
+    clocks = ClockSampler(device)
+    clocks.start()
+    s_lat, s_span, s_samples, s_kept, stats, submit_s, late = served_run(arrivals)
+    ranks.barrier()
+    p_lat, p_span, p_samples, p_kept = plain_run(arrivals)
+    clock_info = clocks.stop()
+    exact = s_samples == p_samples and all(np.array_equal(s_kept[i], p_kept[i]) for i in p_kept)
+
+    capacity = None
+    if args.capacity_requests:
+        m = min(args.capacity_requests, n)
+        at_once = np.zeros(m)
+        ranks.barrier()
+        c_s = served_run(at_once)
+        ranks.barrier()
+        c_p = plain_run(at_once)
+        capacity = {"requests": m, "served_graphs_per_s": ranks.sum(m / ranks.max(c_s[1])),
+                    "plain_graphs_per_s": ranks.sum(m / ranks.max(c_p[1])),
+                    "served_peak_active": c_s[4]["peak_active"]}
+        capacity["speedup_vs_plain"] = capacity["served_graphs_per_s"] / capacity["plain_graphs_per_s"]
+
+    served_gps = ranks.sum(n / ranks.max(s_span))
+    plain_gps = ranks.sum(n / ranks.max(p_span))
+    line = {
+        "metric": f"served graphs/s (Poisson {args.rate:g}/s, {iters} iterations each)", "value": served_gps,
+        "unit": "graphs/s", "n_gpus": ranks.world, "higher_is_better": True, "scaling": "weak", "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": f"served: {n} Poisson requests per rank at {args.rate:g}/s, edges log-uniform "
+                               f"500-50k, grids 512/1024/2048, {iters} iterations, "
+                               f"{args.budget_gb:g} GB admission budget",
+                   "max_active": args.max_active, "max_step": args.max_step,
+                   "fine_cells": {f"{k[0]}px r{k[1]}": v for k, v in tuned.items()},
+                   "parallelism": f"one arrival stream per rank x{ranks.world}"},
+        "latency": pct(s_lat), "plain_latency": pct(p_lat),
+        "plain_graphs_per_s": plain_gps, "speedup_vs_plain": served_gps / plain_gps,
+        "served_points_iter_per_s": ranks.sum(s_samples * iters / s_span),
+        "server": {k: stats[k] for k in ("peak_active", "peak_device_bytes", "budget_waits", "evictions", "steps")},
+        "submit_seconds": submit_s, "arrivals_late": late,
+        "capacity_all_at_once": capacity,
+        "bit_exact_vs_plain": exact,
+        "clocks": clock_info,
+    }
+    if ranks.rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
     ranks = Ranks(args.gpus)
     try:
         if args.impl == "reference":
             run_reference(args, ranks)
+        elif args.workload == "batched":
+            run_batched(args, ranks)
+        elif args.workload == "served":
+            run_served(args, ranks)
         else:
             run_ours(args, ranks)
     finally:

@@ -74,6 +74,32 @@ class _Info(ctypes.Structure):
     ]
 
 
+class _ServerOptions(ctypes.Structure):
+    _fields_ = [
+        ("device", ctypes.c_int32), ("max_active", ctypes.c_uint32), ("budget_bytes", ctypes.c_uint64),
+        ("max_step", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 7),
+    ]
+
+
+class _RequestResult(ctypes.Structure):
+    _fields_ = [
+        ("id", ctypes.c_uint64), ("status", ctypes.c_int32), ("samples", ctypes.c_uint32),
+        ("iterations", ctypes.c_uint32), ("reserved0", ctypes.c_uint32), ("arrival_s", ctypes.c_double),
+        ("admitted_s", ctypes.c_double), ("finished_s", ctypes.c_double), ("device_bytes", ctypes.c_uint64),
+        ("message", ctypes.c_char * 160),
+    ]
+
+
+class _ServerStats(ctypes.Structure):
+    _fields_ = [
+        ("submitted", ctypes.c_uint64), ("finished", ctypes.c_uint64), ("failed", ctypes.c_uint64),
+        ("steps", ctypes.c_uint64), ("rebuilds", ctypes.c_uint64), ("budget_waits", ctypes.c_uint64),
+        ("evictions", ctypes.c_uint64), ("queued", ctypes.c_uint32), ("active", ctypes.c_uint32),
+        ("peak_active", ctypes.c_uint32), ("resident_results", ctypes.c_uint32), ("device_bytes", ctypes.c_uint64),
+        ("peak_device_bytes", ctypes.c_uint64),
+    ]
+
+
 # Every entry point of include/bt.h with its ctypes signature.
 SIGNATURES = {
     "bt_abi_version": ([], ctypes.c_int32),
@@ -101,11 +127,15 @@ SIGNATURES = {
     "bt_distortion": ([_vp, ctypes.c_uint32, _f64p, _f64p], ctypes.c_int32),
     "bt_stage_times": ([_vp, ctypes.POINTER(ctypes.c_char_p), _f32p, ctypes.c_uint32, _u32p], ctypes.c_int32),
     "bt_density_noalloc": ([_vp, _vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_float, _vp], ctypes.c_int32),
+    "bt_autotune": ([ctypes.POINTER(_Options), _f32p, ctypes.c_uint32, _u32p, ctypes.c_uint32, ctypes.c_uint32,
+                     ctypes.POINTER(_Options), _f32p], ctypes.c_int32),
     "bt_batch_create": ([ctypes.c_int32, ctypes.POINTER(_vp)], ctypes.c_int32),
     "bt_batch_destroy": ([_vp], None),
     "bt_batch_last_error": ([_vp], ctypes.c_char_p),
     "bt_batch_add": ([_vp, ctypes.POINTER(_Options), _f32p, ctypes.c_uint32, _u32p, ctypes.c_uint32, _u32p, _u32p],
                      ctypes.c_int32),
+    "bt_batch_add_many": ([_vp, ctypes.c_uint32, ctypes.POINTER(_Options), ctypes.POINTER(_f32p), _u32p,
+                           ctypes.POINTER(_u32p), _u32p, _u32p, _u32p], ctypes.c_int32),
     "bt_batch_remove": ([_vp, ctypes.c_uint32], ctypes.c_int32),
     "bt_batch_iterate": ([_vp, ctypes.c_uint32], ctypes.c_int32),
     "bt_batch_iterate_async": ([_vp, ctypes.c_uint32], ctypes.c_int32),
@@ -113,6 +143,18 @@ SIGNATURES = {
     "bt_batch_iterate_timed": ([_vp, ctypes.c_uint32, _f32p], ctypes.c_int32),
     "bt_batch_slot_count": ([_vp, _u32p, _u32p], ctypes.c_int32),
     "bt_batch_slot": ([_vp, ctypes.c_uint32], _vp),
+    "bt_server_options_init": ([ctypes.POINTER(_ServerOptions)], None),
+    "bt_server_create": ([ctypes.POINTER(_ServerOptions), ctypes.POINTER(_vp)], ctypes.c_int32),
+    "bt_server_destroy": ([_vp], None),
+    "bt_server_last_error": ([_vp], ctypes.c_char_p),
+    "bt_server_clock": ([_vp], ctypes.c_double),
+    "bt_server_submit": ([_vp, ctypes.POINTER(_Options), _f32p, ctypes.c_uint32, _u32p, ctypes.c_uint32,
+                          ctypes.c_uint32, ctypes.c_double, ctypes.POINTER(ctypes.c_uint64)], ctypes.c_int32),
+    "bt_server_next": ([_vp, ctypes.c_double, ctypes.POINTER(_RequestResult)], ctypes.c_int32),
+    "bt_server_read_points": ([_vp, ctypes.c_uint64, _vp, ctypes.c_size_t], ctypes.c_int32),
+    "bt_server_result": ([_vp, ctypes.c_uint64], _vp),
+    "bt_server_release": ([_vp, ctypes.c_uint64], ctypes.c_int32),
+    "bt_server_stats_get": ([_vp, ctypes.POINTER(_ServerStats)], ctypes.c_int32),
     "bt_graph_parse": ([ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(_vp)], ctypes.c_int32),
     "bt_graph_load": ([ctypes.c_char_p, ctypes.POINTER(_vp)], ctypes.c_int32),
     "bt_graph_free": ([_vp], None),
@@ -338,10 +380,18 @@ class Gpu:
         return Info(*(getattr(i, f) for f, _ in _Info._fields_))
 
     # -- readbacks --
-    def read_records(self) -> np.ndarray:
-        """Raw 12-byte {x, y, edge_id} records (sample order)."""
+    def read_records(self, out: np.ndarray | None = None) -> np.ndarray:
+        """Raw 12-byte {x, y, edge_id} records (sample order). `out`, when
+        given, is a C-contiguous host array of at least 12 bytes per sample
+        (pinned memory reads fastest); the view of it that was filled is
+        returned."""
         n = self.info().samples
-        out = np.zeros(n * 12, np.uint8)
+        if out is None:
+            out = np.zeros(n * 12, np.uint8)
+        else:
+            if not out.flags.c_contiguous or out.nbytes < n * 12:
+                raise ValueError("record buffer must be C-contiguous with 12 bytes per sample")
+            out = out.reshape(-1).view(np.uint8)[: n * 12]
         self._ck(library().bt_read_points(self._h, out.ctypes.data, out.size))
         return out
 
@@ -427,6 +477,21 @@ class Gpu:
         return layout.decode(self.read_records())
 
 
+def autotune(options: Options, xy: np.ndarray, starts: np.ndarray, iterations: int = 3) -> tuple[Options, float]:
+    """bt_autotune: the search-cell size that iterates this graph fastest.
+    Returns the tuned options and the time of `iterations` iterations (ms)."""
+    import dataclasses
+
+    xy = np.ascontiguousarray(xy, np.float32)
+    starts = np.ascontiguousarray(starts, np.uint32)
+    o = options._struct()
+    tuned = _Options()
+    ms = np.zeros(1, np.float32)
+    _check(library().bt_autotune(ctypes.byref(o), _p(xy, _f32p), xy.size // 2, _p(starts, _u32p), starts.size,
+                                 iterations, ctypes.byref(tuned), _p(ms, _f32p)))
+    return dataclasses.replace(options, fine_cells=int(tuned.fine_cells)), float(ms[0])
+
+
 class _SlotView(Gpu):
     """Read-only view of a batch slot's context (owned by the batch)."""
 
@@ -475,6 +540,26 @@ class Batch:
         self._options[slot.value] = options
         return slot.value, n.value
 
+    def add_many(self, jobs) -> list[tuple[int, int]]:
+        """Upload (options, xy, starts) triples concurrently; returns
+        [(slot, samples)] in order."""
+        jobs = list(jobs)
+        n = len(jobs)
+        opts = (_Options * n)(*[o._struct() for o, _, _ in jobs])
+        xys = [np.ascontiguousarray(xy, np.float32) for _, xy, _ in jobs]
+        sts = [np.ascontiguousarray(st, np.uint32) for _, _, st in jobs]
+        xy_ptrs = (_f32p * n)(*[_p(a, _f32p) for a in xys])
+        st_ptrs = (_u32p * n)(*[_p(a, _u32p) for a in sts])
+        n_points = np.array([a.size // 2 for a in xys], np.uint32)
+        n_starts = np.array([a.size for a in sts], np.uint32)
+        slots = np.zeros(n, np.uint32)
+        samples = np.zeros(n, np.uint32)
+        self._ck(library().bt_batch_add_many(self._h, n, opts, xy_ptrs, _p(n_points, _u32p), st_ptrs,
+                                             _p(n_starts, _u32p), _p(slots, _u32p), _p(samples, _u32p)))
+        for (o, _, _), s in zip(jobs, slots.tolist()):
+            self._options[s] = o
+        return list(zip(slots.tolist(), samples.tolist()))
+
     def remove(self, slot: int) -> None:
         self._ck(library().bt_batch_remove(self._h, slot))
         self._options.pop(slot, None)
@@ -505,6 +590,110 @@ class Batch:
         if not h:
             raise BtError(3, library().bt_batch_last_error(self._h).decode())
         return _SlotView(h, self._options[slot])
+
+
+@dataclass
+class RequestResult:
+    """A finished (or failed) serving request; times are on the server clock."""
+    id: int
+    status: int
+    samples: int
+    iterations: int
+    arrival_s: float
+    admitted_s: float
+    finished_s: float
+    device_bytes: int
+    message: str
+
+    @property
+    def latency_s(self) -> float:
+        return self.finished_s - self.arrival_s
+
+
+class Server:
+    """Continuous batching of arriving requests (bt_server_*): a native worker
+    thread admits requests by a device-memory budget, uploads them while the
+    batch iterates, and frees each batch slot as soon as that graph's own
+    iteration count is reached. Results stay on the device until released."""
+
+    def __init__(self, device: int = 0, max_active: int = 32, budget_bytes: int = 120_000_000_000,
+                 max_step: int = 1):
+        o = _ServerOptions()
+        library().bt_server_options_init(ctypes.byref(o))
+        o.device, o.max_active, o.budget_bytes, o.max_step = device, max_active, budget_bytes, max_step
+        h = _vp()
+        _check(library().bt_server_create(ctypes.byref(o), ctypes.byref(h)))
+        self._h = h
+        self._options: dict[int, Options] = {}
+
+    def close(self) -> None:
+        h = getattr(self, "_h", None)
+        if h and _lib is not None:
+            _lib.bt_server_destroy(h)
+        self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def _ck(self, status: int) -> None:
+        if status:
+            msg = library().bt_server_last_error(self._h)
+            raise BtError(status, msg.decode() if msg else "")
+
+    def clock(self) -> float:
+        return library().bt_server_clock(self._h)
+
+    def submit(self, options: Options, xy: np.ndarray, starts: np.ndarray, iterations: int,
+               arrival_s: float | None = None) -> int:
+        """Queue a request (the inputs are copied); returns its id."""
+        xy = np.ascontiguousarray(xy, np.float32)
+        starts = np.ascontiguousarray(starts, np.uint32)
+        o = options._struct()
+        rid = ctypes.c_uint64()
+        self._ck(library().bt_server_submit(self._h, ctypes.byref(o), _p(xy, _f32p), xy.size // 2,
+                                            _p(starts, _u32p), starts.size, iterations,
+                                            -1.0 if arrival_s is None else float(arrival_s), ctypes.byref(rid)))
+        self._options[rid.value] = options
+        return rid.value
+
+    def next(self, timeout_s: float = 60.0) -> RequestResult:
+        """The next request to finish, in completion order."""
+        r = _RequestResult()
+        self._ck(library().bt_server_next(self._h, timeout_s, ctypes.byref(r)))
+        return RequestResult(r.id, r.status, r.samples, r.iterations, r.arrival_s, r.admitted_s, r.finished_s,
+                             r.device_bytes, r.message.decode())
+
+    def read_records(self, rid: int, samples: int, out: np.ndarray | None = None) -> np.ndarray:
+        """12-byte {x, y, edge_id} records of a finished request."""
+        n = 12 * samples
+        if out is None:
+            out = np.zeros(n, np.uint8)
+        else:
+            if not out.flags.c_contiguous or out.nbytes < n:
+                raise ValueError("record buffer must be C-contiguous with 12 bytes per sample")
+            out = out.reshape(-1).view(np.uint8)[:n]
+        self._ck(library().bt_server_read_points(self._h, rid, out.ctypes.data, n))
+        return out
+
+    def read_points(self, rid: int, samples: int) -> tuple[np.ndarray, np.ndarray]:
+        rec = self.read_records(rid, samples).view(np.uint32).reshape(-1, 3)
+        return rec[:, :2].copy().view(np.float32), rec[:, 2].copy()
+
+    def result(self, rid: int) -> Gpu:
+        """A finished request's context for readbacks until it is released."""
+        h = library().bt_server_result(self._h, rid)
+        if not h:
+            raise BtError(3, "no finished request with this id")
+        return _SlotView(h, self._options[rid])
+
+    def release(self, rid: int) -> None:
+        self._ck(library().bt_server_release(self._h, rid))
+        self._options.pop(rid, None)
+
+    def stats(self) -> dict:
+        st = _ServerStats()
+        self._ck(library().bt_server_stats_get(self._h, ctypes.byref(st)))
+        return {name: getattr(st, name) for name, _ in _ServerStats._fields_}
 
 
 @dataclass

@@ -498,6 +498,39 @@ bt_status need_slot(bt_batch* b, uint32_t slot, bt_ctx** c) {
 }
 
 }  // namespace
+
+bt_status batch_attach(bt_batch* b, bt_ctx* c, uint32_t* slot) {
+    if (!b || !c || !slot) return bfail(b, BT_ERR_INVALID, "null argument");
+    if (!c->uploaded || !c->has_grid)
+        return bfail(b, BT_ERR_INVALID, "a batch slot needs an uploaded graph with a neighbour radius");
+    if (c->device != b->device) return bfail(b, BT_ERR_INVALID, "the graph lives on another device");
+    if ((c->cells + kCellTile - 1) / kCellTile > kMaxCellTiles)
+        return bfail(b, BT_ERR_INVALID, "search grid too large for a batch slot (over 1M search cells)");
+    // Reuse a free slot index, else append.
+    uint32_t idx = 0;
+    while (idx < b->slots.size() && b->slots[idx].active) ++idx;
+    if (idx == b->slots.size()) b->slots.emplace_back();
+    Slot& s = b->slots[idx];
+    if (s.ctx) bt_destroy(s.ctx);
+    s.ctx = c;
+    s.active = true;
+    s.taps_count = 0;
+    b->dirty = true;
+    *slot = idx;
+    return BT_OK;
+}
+
+bt_ctx* batch_detach(bt_batch* b, uint32_t slot) {
+    bt_ctx* c = nullptr;
+    if (need_slot(b, slot, &c)) return nullptr;
+    cudaSetDevice(b->device);
+    if (bwait(b)) return nullptr;
+    b->slots[slot].active = false;
+    b->slots[slot].ctx = nullptr;
+    b->dirty = true;
+    return c;
+}
+
 }  // namespace bt
 
 using namespace bt;
@@ -605,21 +638,49 @@ bt_status bt_batch_add(bt_batch* b, const bt_options* options, const float* xy, 
         bt_destroy(c);
         return bfail(b, s, msg);
     }
-    if ((c->cells + kCellTile - 1) / kCellTile > kMaxCellTiles) {
+    if (bt_status s = batch_attach(b, c, slot)) {
         bt_destroy(c);
-        return bfail(b, BT_ERR_INVALID, "search grid too large for a batch slot (over 1M search cells)");
+        return s;
     }
-    // Reuse a free slot index, else append.
-    uint32_t idx = 0;
-    while (idx < b->slots.size() && b->slots[idx].active) ++idx;
-    if (idx == b->slots.size()) b->slots.emplace_back();
-    Slot& s = b->slots[idx];
-    if (s.ctx) bt_destroy(s.ctx);
-    s.ctx = c;
-    s.active = true;
-    s.taps_count = 0;
-    b->dirty = true;
-    *slot = idx;
+    return BT_OK;
+}
+
+bt_status bt_batch_add_many(bt_batch* b, uint32_t count, const bt_options* options, const float* const* xy,
+                            const uint32_t* n_points, const uint32_t* const* starts, const uint32_t* n_starts,
+                            uint32_t* slots, uint32_t* samples) {
+    if (!b || (count && (!options || !xy || !n_points || !starts || !n_starts || !slots || !samples)))
+        return bfail(b, BT_ERR_INVALID, "null argument");
+    std::vector<bt_ctx*> ctxs(count, nullptr);
+    auto unwind = [&](bt_status s, std::string msg) {   // by value: msg may live in a context destroyed here
+        for (bt_ctx* c : ctxs) bt_destroy(c);
+        return bfail(b, s, msg);
+    };
+    for (uint32_t i = 0; i < count; ++i) {
+        if (options[i].neighbor_radius == 0) return unwind(BT_ERR_NOT_CONFIGURED, "neighbor radius is not configured");
+        bt_options o = options[i];
+        o.device = b->device;
+        o.timing = 0;
+        if (bt_status s = bt_create(&o, &ctxs[i])) return unwind(s, bt_last_error(nullptr));
+    }
+    // Every graph's phase on its own stream, one host wait per phase.
+    for (uint32_t i = 0; i < count; ++i)
+        if (bt_status s = upload_begin(ctxs[i], xy[i], n_points[i], starts[i], n_starts[i]))
+            return unwind(s, ctxs[i]->err);
+    for (uint32_t i = 0; i < count; ++i)
+        if (bt_status s = upload_wait(ctxs[i])) return unwind(s, ctxs[i]->err);
+    for (uint32_t i = 0; i < count; ++i)
+        if (bt_status s = upload_finish(ctxs[i])) return unwind(s, ctxs[i]->err);
+    for (uint32_t i = 0; i < count; ++i)
+        if (bt_status s = upload_wait(ctxs[i])) return unwind(s, ctxs[i]->err);
+    for (uint32_t i = 0; i < count; ++i) {
+        if (bt_status s = upload_check(ctxs[i], &samples[i])) return unwind(s, ctxs[i]->err);
+        if ((ctxs[i]->cells + kCellTile - 1) / kCellTile > kMaxCellTiles)
+            return unwind(BT_ERR_INVALID, "search grid too large for a batch slot (over 1M search cells)");
+    }
+    for (uint32_t i = 0; i < count; ++i) {
+        batch_attach(b, ctxs[i], &slots[i]);   // cannot fail: every check above passed
+        ctxs[i] = nullptr;
+    }
     return BT_OK;
 }
 

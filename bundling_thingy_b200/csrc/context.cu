@@ -52,6 +52,15 @@ bt_status cuda_fail(bt_ctx* c, cudaError_t e, const char* what) {
 bt_status ensure(bt_ctx* c, DevBuf& b, size_t bytes) {
     if (bytes == 0) bytes = 16;
     if (b.bytes >= bytes) return BT_OK;
+    const uint64_t growth = bytes - b.bytes;
+    if (c->account) {
+        // Charge the growth before allocating; give it back on failure.
+        uint64_t used = c->account->used.load();
+        do {
+            if (used + growth > c->account->limit)
+                return fail(c, BT_ERR_BUDGET, "device memory budget of the server is exhausted");
+        } while (!c->account->used.compare_exchange_weak(used, used + growth));
+    }
     if (b.p) {
         cudaFree(b.p);
         c->device_bytes -= b.bytes;
@@ -61,6 +70,7 @@ bt_status ensure(bt_ctx* c, DevBuf& b, size_t bytes) {
     cudaError_t e = cudaMalloc(&b.p, bytes);
     if (e != cudaSuccess) {
         cudaGetLastError();
+        if (c->account) c->account->used -= bytes;   // the old buffer is gone too
         return cuda_fail(c, e, "device allocation");
     }
     b.bytes = bytes;
@@ -284,13 +294,43 @@ void bt_options_init(bt_options* o) {
 
 const char* bt_last_error(const bt_ctx* ctx) { return ctx ? ctx->err.c_str() : g_thread_error.c_str(); }
 
-bt_status bt_create(const bt_options* options, bt_ctx** out) {
+bt_status bt_create(const bt_options* options, bt_ctx** out) { return bt::create_context(options, nullptr, out); }
+
+void bt_destroy(bt_ctx* c) {
+    if (!c) return;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    drop_graphs(c);
+    DevBuf* bufs[] = {&c->cp, &c->starts, &c->packed, &c->offsets, &c->scan64, &c->edges, &c->paths, &c->totals,
+                      &c->status, &c->edge_ids, &c->segments, &c->tmp_xy, &c->tmp_tag, &c->tmp_cell,
+                      &c->neighbors, &c->baseline, &c->current, &c->sorted_rec[0], &c->sorted_rec[1],
+                      &c->cellsum, &c->cell_prefix, &c->sorted_tag[0], &c->sorted_tag[1], &c->hist,
+                      &c->cell_start, &c->table_scratch, &c->counts, &c->himg, &c->vimg, &c->norm, &c->peak,
+                      &c->records, &c->integrals};
+    for (DevBuf* b : bufs) release(*b);
+    if (c->account) c->account->used -= c->device_bytes;
+    for (StageRec& r : c->stage_pool) {
+        cudaEventDestroy(r.start);
+        cudaEventDestroy(r.stop);
+    }
+    if (c->h_totals) cudaFreeHost(c->h_totals);
+    if (c->h_status) cudaFreeHost(c->h_status);
+    if (c->done) cudaEventDestroy(c->done);
+    if (c->t0) cudaEventDestroy(c->t0);
+    if (c->t1) cudaEventDestroy(c->t1);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+}  // extern "C"
+
+bt_status bt::create_context(const bt_options* options, bt::MemAccount* account, bt_ctx** out) {
     if (!options || !out) return fail(nullptr, BT_ERR_INVALID, "null argument");
     *out = nullptr;
     if (bt_status s = validate_options(options, nullptr)) return s;
     auto* c = new bt_ctx();
     c->opt = *options;
     c->device = options->device;
+    c->account = account;
     auto bail = [&](bt_status s) {
         std::string msg = c->err;
         bt_destroy(c);
@@ -373,34 +413,14 @@ bt_status bt_create(const bt_options* options, bt_ctx** out) {
     return BT_OK;
 }
 
-void bt_destroy(bt_ctx* c) {
-    if (!c) return;
-    if (c->stream) cudaStreamSynchronize(c->stream);
-    drop_graphs(c);
-    DevBuf* bufs[] = {&c->cp, &c->starts, &c->packed, &c->offsets, &c->scan64, &c->edges, &c->paths, &c->totals,
-                      &c->status, &c->edge_ids, &c->segments, &c->tmp_xy, &c->tmp_tag, &c->tmp_cell,
-                      &c->neighbors, &c->baseline, &c->current, &c->sorted_rec[0], &c->sorted_rec[1],
-                      &c->cellsum, &c->cell_prefix, &c->sorted_tag[0], &c->sorted_tag[1], &c->hist,
-                      &c->cell_start, &c->table_scratch, &c->counts, &c->himg, &c->vimg, &c->norm, &c->peak,
-                      &c->records, &c->integrals};
-    for (DevBuf* b : bufs) release(*b);
-    for (StageRec& r : c->stage_pool) {
-        cudaEventDestroy(r.start);
-        cudaEventDestroy(r.stop);
-    }
-    if (c->h_totals) cudaFreeHost(c->h_totals);
-    if (c->h_status) cudaFreeHost(c->h_status);
-    if (c->done) cudaEventDestroy(c->done);
-    if (c->t0) cudaEventDestroy(c->t0);
-    if (c->t1) cudaEventDestroy(c->t1);
-    if (c->stream) cudaStreamDestroy(c->stream);
-    delete c;
-}
-
-bt_status bt_upload(bt_ctx* c, const float* xy, uint32_t n_points, const uint32_t* starts, uint32_t n_starts,
-                    uint32_t* out_samples) {
+// Gpu::upload in three phases so that a batch can run many uploads
+// concurrently with two host waits in total: begin (validate, copy in, count
+// kernel, totals read back asynchronously) — wait — finish (offsets, emit,
+// density, first binning, status read back) — wait — check.
+bt_status bt::upload_begin(bt_ctx* c, const float* xy, uint32_t n_points, const uint32_t* starts,
+                           uint32_t n_starts) {
     if (!c) return fail(nullptr, BT_ERR_INVALID, "null context");
-    if (!xy || !starts || !out_samples) return fail(c, BT_ERR_INVALID, "null argument");
+    if (!xy || !starts) return fail(c, BT_ERR_INVALID, "null argument");
     cudaSetDevice(c->device);
     // The previous graph is released first (gpu.rs:494-497).
     c->uploaded = false;
@@ -456,13 +476,14 @@ bt_status bt_upload(bt_ctx* c, const float* xy, uint32_t n_points, const uint32_
     BT_CUDA(c, cudaMemsetAsync(c->totals.p, 0, 32, c->stream));
     BT_CUDA(c, cudaMemsetAsync(c->status.p, 0, 16, c->stream));
 
-    const bt::Norm norm{nm[0], nm[1], nm[2], nm[3], nm[4]};
+    c->norm_params = bt::Norm{nm[0], nm[1], nm[2], nm[3], nm[4]};
+    c->n_paths = E;
     stage_begin(c, "graph.count");
     bt::ResampleCountArgs ca{};
     ca.cp = c->cp.as<float2>();
     ca.starts = c->starts.as<uint32_t>();
     ca.paths = E;
-    ca.norm = norm;
+    ca.norm = c->norm_params;
     ca.sx = c->rsx;
     ca.sy = c->rsy;
     ca.capacity = c->capacity;
@@ -472,7 +493,13 @@ bt_status bt_upload(bt_ctx* c, const float* xy, uint32_t n_points, const uint32_
     bt::launch_resample_count(ca, c->stream);
     stage_end(c);
     BT_CUDA(c, cudaMemcpyAsync(c->h_totals, c->totals.p, 16, cudaMemcpyDeviceToHost, c->stream));
-    if (bt_status s = wait(c)) return s;
+    return BT_OK;
+}
+
+bt_status bt::upload_finish(bt_ctx* c) {
+    cudaSetDevice(c->device);
+    const uint32_t E = c->n_paths;
+    const bt::Norm norm = c->norm_params;
     const unsigned long long total = c->h_totals[0], drawn = c->h_totals[1];
     // count_paths overflow 1 (resampling.wgsl:151-156), PendingGraph::finish (resampling.rs:294-308).
     if (total > c->capacity)
@@ -484,11 +511,8 @@ bt_status bt_upload(bt_ctx* c, const float* xy, uint32_t n_points, const uint32_
     const uint32_t N = static_cast<uint32_t>(total);
     const uint32_t segs = static_cast<uint32_t>(total - drawn);
 
-    stage_begin(c, "graph.emit");
-    bt::exclusive_scan<unsigned long long>(c->packed.as<unsigned long long>(), c->offsets.as<unsigned long long>(), E,
-                                           c->scan64.as<unsigned long long>(), c->stream);
-    bt::launch_paths_from_scan(c->packed.as<unsigned long long>(), c->offsets.as<unsigned long long>(), E,
-                               c->paths.as<bt::PathRec>(), c->stream);
+    // Every allocation before the first launch, so that a phase refused by a
+    // memory budget launched nothing and can be retried.
     if (bt_status s = ensure(c, c->edge_ids, 4ull * N)) return s;
     if (bt_status s = ensure(c, c->segments, 4ull * segs)) return s;
     if (bt_status s = ensure(c, c->tmp_xy, 8ull * N)) return s;
@@ -501,11 +525,19 @@ bt_status bt_upload(bt_ctx* c, const float* xy, uint32_t n_points, const uint32_
         }
         if (c->opt.record_neighbors)
             if (bt_status s = ensure(c, c->neighbors, 4ull * N)) return s;
-        BT_CUDA(c, cudaMemsetAsync(c->hist.p, 0, c->cells * 4, c->stream));
-        BT_CUDA(c, cudaMemsetAsync(c->cellsum.p, 0, c->cells * sizeof(bt::LL2), c->stream));
     }
     if (c->opt.evaluate_distortion)
         if (bt_status s = ensure(c, c->baseline, 8ull * N)) return s;
+
+    stage_begin(c, "graph.emit");
+    bt::exclusive_scan<unsigned long long>(c->packed.as<unsigned long long>(), c->offsets.as<unsigned long long>(), E,
+                                           c->scan64.as<unsigned long long>(), c->stream);
+    bt::launch_paths_from_scan(c->packed.as<unsigned long long>(), c->offsets.as<unsigned long long>(), E,
+                               c->paths.as<bt::PathRec>(), c->stream);
+    if (c->has_grid) {
+        BT_CUDA(c, cudaMemsetAsync(c->hist.p, 0, c->cells * 4, c->stream));
+        BT_CUDA(c, cudaMemsetAsync(c->cellsum.p, 0, c->cells * sizeof(bt::LL2), c->stream));
+    }
     if (c->accumulate) {
         BT_CUDA(c, cudaMemsetAsync(c->counts.p, 0, c->texels * 4, c->stream));
         BT_CUDA(c, cudaMemsetAsync(c->peak.p, 0, 4, c->stream));
@@ -545,12 +577,51 @@ bt_status bt_upload(bt_ctx* c, const float* xy, uint32_t n_points, const uint32_
         c->cur = 0;
     }
     BT_CUDA(c, cudaMemcpyAsync(c->h_status, c->status.p, 4, cudaMemcpyDeviceToHost, c->stream));
-    if (bt_status s = wait(c)) return s;
+    return BT_OK;
+}
+
+bt_status bt::upload_check(bt_ctx* c, uint32_t* out_samples) {
     if (c->h_status[0] & 2u) return fail(c, BT_ERR_MISMATCH, "GPU resampling count and write passes disagree");
     if (c->h_status[0] & 8u) return fail(c, BT_ERR_CUDA, "inconsistent neighbour-grid binning");
     c->uploaded = true;
-    *out_samples = N;
+    *out_samples = c->samples;
     return BT_OK;
+}
+
+bt_status bt::upload_wait(bt_ctx* c) { return wait(c); }
+
+bt_status bt::copy_records(bt_ctx* c, void* dst, size_t bytes) {
+    if (!dst || bytes != 12ull * c->samples) return fail(c, BT_ERR_INVALID, "point buffer must hold 12 bytes per sample");
+    cudaSetDevice(c->device);
+    BT_CUDA(c, cudaMemcpyAsync(dst, c->records.p, bytes, cudaMemcpyDeviceToHost, c->stream));
+    return wait(c);
+}
+
+bt_status bt::reserve_records(bt_ctx* c) { return ensure(c, c->records, 12ull * c->samples); }
+
+bt_status bt::prepare_records(bt_ctx* c) {
+    cudaSetDevice(c->device);
+    if (bt_status s = ensure(c, c->records, 12ull * c->samples)) return s;
+    if (c->has_grid) {
+        bt::launch_unsort_records(c->sorted_rec[c->cur].as<uint4>(), c->sorted_tag[c->cur].as<uint32_t>(),
+                                  c->edge_ids.as<uint32_t>(), c->samples, c->records.as<uint32_t>(), c->stream);
+    } else {
+        bt::launch_records_from_sample_order(c->tmp_xy.as<float2>(), c->edge_ids.as<uint32_t>(), c->samples,
+                                             c->records.as<uint32_t>(), c->stream);
+    }
+    return BT_OK;
+}
+
+extern "C" {
+
+bt_status bt_upload(bt_ctx* c, const float* xy, uint32_t n_points, const uint32_t* starts, uint32_t n_starts,
+                    uint32_t* out_samples) {
+    if (!out_samples) return fail(c, BT_ERR_INVALID, "null argument");
+    if (bt_status s = bt::upload_begin(c, xy, n_points, starts, n_starts)) return s;
+    if (bt_status s = wait(c)) return s;
+    if (bt_status s = bt::upload_finish(c)) return s;
+    if (bt_status s = wait(c)) return s;
+    return bt::upload_check(c, out_samples);
 }
 
 bt_status bt_upload_graph(bt_ctx* c, const bt_graph* g, uint32_t* out_samples) {
@@ -639,6 +710,47 @@ bt_status bt_iterate_timed(bt_ctx* c, uint32_t n, float* device_ms) {
     return check_iteration_status(c);
 }
 
+bt_status bt_autotune(const bt_options* options, const float* xy, uint32_t n_points, const uint32_t* starts,
+                      uint32_t n_starts, uint32_t iterations, bt_options* tuned, float* best_ms) {
+    if (!options || !tuned) return fail(nullptr, BT_ERR_INVALID, "null argument");
+    *tuned = *options;
+    if (best_ms) *best_ms = 0.0f;
+    const uint32_t r = options->neighbor_radius;
+    if (r == 0 || iterations == 0) return BT_OK;
+    std::vector<uint32_t> candidates;
+    for (uint32_t k : {std::max(1u, r / 4u), std::max(1u, r / 2u), r, 2u * r})
+        if (k <= 4096 && std::find(candidates.begin(), candidates.end(), k) == candidates.end())
+            candidates.push_back(k);
+    float best = -1.0f;
+    for (uint32_t k : candidates) {
+        bt_options o = *options;
+        o.fine_cells = k;
+        o.timing = 0;
+        o.use_graphs = 1;
+        bt_ctx* c = nullptr;
+        if (bt_status s = bt_create(&o, &c)) return s;
+        uint32_t samples = 0;
+        float ms = 0.0f;
+        bt_status s = bt_upload(c, xy, n_points, starts, n_starts, &samples);
+        if (!s) s = bt_iterate(c, 1);
+        if (!s) s = bt_iterate_timed(c, iterations, &ms);
+        if (s) {
+            std::string msg = c->err;
+            bt_destroy(c);
+            return fail(nullptr, s, msg);
+        }
+        bt_destroy(c);
+        if (best < 0.0f || ms < best) {
+            best = ms;
+            *tuned = o;
+        }
+    }
+    tuned->timing = options->timing;
+    tuned->use_graphs = options->use_graphs;
+    if (best_ms) *best_ms = best;
+    return BT_OK;
+}
+
 bt_status bt_get_info(bt_ctx* c, bt_info* info) {
     if (!c || !info) return fail(c, BT_ERR_INVALID, "null argument");
     std::memset(info, 0, sizeof(*info));
@@ -689,14 +801,7 @@ bt_status current_positions(bt_ctx* c, const float2** out) {
 bt_status bt_read_points(bt_ctx* c, void* dst, size_t bytes) {
     if (bt_status s = need_graph(c)) return s;
     if (!dst || bytes != 12ull * c->samples) return fail(c, BT_ERR_INVALID, "point buffer must hold 12 bytes per sample");
-    if (bt_status s = ensure(c, c->records, 12ull * c->samples)) return s;
-    if (c->has_grid) {
-        bt::launch_unsort_records(c->sorted_rec[c->cur].as<uint4>(), c->sorted_tag[c->cur].as<uint32_t>(),
-                                  c->edge_ids.as<uint32_t>(), c->samples, c->records.as<uint32_t>(), c->stream);
-    } else {
-        bt::launch_records_from_sample_order(c->tmp_xy.as<float2>(), c->edge_ids.as<uint32_t>(), c->samples,
-                                             c->records.as<uint32_t>(), c->stream);
-    }
+    if (bt_status s = bt::prepare_records(c)) return s;
     return copy_out(c, dst, c->records.p, bytes);
 }
 

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <string>
 #include <vector>
 
@@ -36,6 +37,41 @@ void set_thread_error(const char* message);
 
 }  // namespace bt
 
+struct bt_ctx;
+
+struct bt_batch;
+
+namespace bt {
+// Device-memory account shared by many contexts: every allocation a context
+// makes is charged against `limit` before it is made, and fails with
+// BT_ERR_BUDGET (nothing allocated) when it would not fit.
+struct MemAccount {
+    std::atomic<uint64_t> used{0};
+    uint64_t limit = 0;
+};
+
+// bt_create with an optional shared account (nullptr = unaccounted).
+bt_status create_context(const bt_options* options, MemAccount* account, bt_ctx** out);
+
+// Gpu::upload in phases (bt_upload = begin, wait, finish, wait, check). A
+// phase that fails with BT_ERR_BUDGET before launching work may be retried.
+bt_status upload_begin(bt_ctx* c, const float* xy, uint32_t n_points, const uint32_t* starts, uint32_t n_starts);
+bt_status upload_finish(bt_ctx* c);
+bt_status upload_check(bt_ctx* c, uint32_t* out_samples);
+bt_status upload_wait(bt_ctx* c);
+
+// Unsort the current positions into 12-byte records on the context's stream
+// (what bt_read_points copies out), and the copy itself.
+bt_status reserve_records(bt_ctx* c);   // the records buffer alone
+bt_status prepare_records(bt_ctx* c);
+bt_status copy_records(bt_ctx* c, void* dst, size_t bytes);
+
+// Hand an uploaded context to a batch (the batch advances it from then on)
+// and take it back without destroying it; detach waits for the batch.
+bt_status batch_attach(bt_batch* b, bt_ctx* c, uint32_t* slot);
+bt_ctx* batch_detach(bt_batch* b, uint32_t slot);
+}  // namespace bt
+
 struct bt_graph {
     bt::HostGraph g;
 };
@@ -64,8 +100,10 @@ struct bt_ctx {
     unsigned long long* h_totals = nullptr;   // pinned
     uint32_t* h_status = nullptr;             // pinned
     size_t device_bytes = 0;
+    bt::MemAccount* account = nullptr;          // shared budget (serving), or none
 
     bool uploaded = false;
+    bt::Norm norm_params{};   // normalisation of the graph being uploaded
     uint32_t samples = 0, n_paths = 0, drawn = 0, capacity = 0;
     uint64_t reserved_bytes = 0;
     uint32_t iterations = 0, density_passes = 0;

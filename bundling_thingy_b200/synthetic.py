@@ -59,24 +59,23 @@ def _weighted_pairs(rng, nodes, n_edges, scale=0.3):
     n = len(nodes)
     if n * (n - 1) // 2 < n_edges:
         raise ValueError("not enough node pairs")
-    seen = set()
-    out = []
-    while len(out) < n_edges:
-        m = max(4 * (n_edges - len(out)), 1024)
+    keys = np.zeros(0, np.int64)   # accepted pairs as lo * n + hi, draw order
+    while True:
+        m = max(4 * (n_edges - keys.size), 1024)
         i = rng.integers(0, n, size=m)
         j = rng.integers(0, n, size=m)
         u = rng.random(size=m)
         d = np.hypot(*(nodes[i] - nodes[j]).T)
         ok = (i != j) & (u < np.exp(-d / scale))
-        for a, b in zip(i[ok].tolist(), j[ok].tolist()):
-            key = (a, b) if a < b else (b, a)
-            if key in seen:
-                continue
-            seen.add(key)
-            out.append(key)
-            if len(out) == n_edges:
-                break
-    return np.array(out, dtype=np.int64)
+        lo, hi = np.minimum(i[ok], j[ok]), np.maximum(i[ok], j[ok])
+        keys = np.concatenate([keys, lo.astype(np.int64) * n + hi])
+        # Keep each pair's first draw, in draw order.
+        _, first = np.unique(keys, return_index=True)
+        keys = keys[np.sort(first)]
+        if keys.size >= n_edges:
+            keys = keys[:n_edges]
+            break
+    return np.stack([keys // n, keys % n], axis=1)
 
 
 def mixture_graph(n_nodes, n_components, n_edges, seed):

@@ -168,6 +168,14 @@ bt_status bt_distortion(bt_ctx* ctx, uint32_t size, double* distortion, double* 
  * entries; returns the number of stages in *count. */
 bt_status bt_stage_times(bt_ctx* ctx, const char** names, float* ms, uint32_t capacity, uint32_t* count);
 
+/* Autotuner (beyond the reference): times `iterations` iterations of this
+ * graph (after one warm-up iteration, CUDA events on the context's stream)
+ * for each candidate search-cell size — 1/4, 1/2, 1 and 2 search cells per
+ * texel of radius — and writes the fastest options to *tuned (its time to
+ * *best_ms when not NULL). Every candidate gives bit-identical results. */
+bt_status bt_autotune(const bt_options* options, const float* xy, uint32_t n_points, const uint32_t* starts,
+                      uint32_t n_starts, uint32_t iterations, bt_options* tuned, float* best_ms);
+
 /* ---- Batches: many independent graphs per launch ----
  *
  * Beyond the reference (which bundles one graph at a time, src/main.rs:113-126):
@@ -185,6 +193,12 @@ const char* bt_batch_last_error(const bt_batch* batch);
  * must be set) into a free slot; returns its slot index and sample count. */
 bt_status bt_batch_add(bt_batch* batch, const bt_options* options, const float* xy, uint32_t n_points,
                        const uint32_t* starts, uint32_t n_starts, uint32_t* slot, uint32_t* samples);
+/* Uploads `count` graphs at once (arrays of per-graph arguments as in
+ * bt_batch_add): every graph's upload runs on its own stream with two host
+ * waits in total. All or nothing: on failure no slot is added. */
+bt_status bt_batch_add_many(bt_batch* batch, uint32_t count, const bt_options* options, const float* const* xy,
+                            const uint32_t* n_points, const uint32_t* const* starts, const uint32_t* n_starts,
+                            uint32_t* slots, uint32_t* samples);
 /* Releases a slot (its index may be reused by a later add). */
 bt_status bt_batch_remove(bt_batch* batch, uint32_t slot);
 /* n iterations of every active slot; waits for the device. */
@@ -197,6 +211,80 @@ bt_status bt_batch_slot_count(bt_batch* batch, uint32_t* active, uint32_t* capac
 /* The context of a slot, for the bt_read_* and bt_get_info calls; owned by
  * the batch (do not destroy or iterate it). Waits for the batch's work. */
 bt_ctx* bt_batch_slot(bt_batch* batch, uint32_t slot);
+
+/* ---- Serving: continuous batching of arriving requests ----
+ *
+ * Beyond the reference (its CLI bundles one graph per process run,
+ * src/main.rs:113-126). A worker thread owns one bt_batch. Submitted requests
+ * become visible at their arrival time; the worker admits them in arrival
+ * order while the device-memory budget and `max_active` allow, uploads every
+ * admitted graph concurrently on its own stream while the batch iterates,
+ * joins them to the batch between iterations, and takes each graph out of the
+ * batch the moment its own iteration count is reached. Admission generalises
+ * Allocation::new (src/resampling.rs:321-397) from one graph to all resident
+ * graphs: every device allocation any request makes is charged against
+ * `budget_bytes` before it is made; a request that does not fit waits (idle
+ * pooled contexts are freed first) until resident graphs finish or results
+ * are released, and fails with BT_ERR_BUDGET only when it does not fit alone.
+ * Results stay on the device until read and released, and equal a standalone
+ * bt_ctx run of the same graph bit for bit. All calls are thread-safe. */
+typedef struct bt_server bt_server;
+
+typedef struct bt_server_options {
+    int32_t device;
+    uint32_t max_active;      /* graphs uploading or iterating at once (0 = unlimited) */
+    uint64_t budget_bytes;    /* device memory of all resident graphs and pooled contexts */
+    uint32_t max_step;        /* batch iterations between admission points (>= 1) */
+    uint32_t reserved[7];
+} bt_server_options;
+
+typedef struct bt_request_result {
+    uint64_t id;
+    int32_t status;           /* BT_OK, or why the request failed */
+    uint32_t samples;
+    uint32_t iterations;
+    uint32_t reserved0;
+    double arrival_s;         /* server clock (seconds since bt_server_create) */
+    double admitted_s;        /* upload started */
+    double finished_s;        /* results ready on the device, batch slot freed */
+    uint64_t device_bytes;    /* device memory the request's graph held */
+    char message[160];
+} bt_request_result;
+
+typedef struct bt_server_stats {
+    uint64_t submitted, finished, failed;
+    uint64_t steps, rebuilds, budget_waits, evictions;
+    uint32_t queued, active, peak_active, resident_results;
+    uint64_t device_bytes, peak_device_bytes;
+} bt_server_stats;
+
+/* device 0, max_active 32, budget 120 GB (120e9 bytes), max_step 1. */
+void bt_server_options_init(bt_server_options* options);
+bt_status bt_server_create(const bt_server_options* options, bt_server** out);
+/* Stops the worker; unfinished requests are dropped. */
+void bt_server_destroy(bt_server* server);
+const char* bt_server_last_error(const bt_server* server);
+/* Seconds since bt_server_create (the clock of arrival and result times). */
+double bt_server_clock(const bt_server* server);
+/* Copies the graph and queues it: `iterations` bt_iterate steps with
+ * `options` (neighbor_radius must be set). The request arrives at
+ * `arrival_s` on the server clock (a negative value = now; a future time
+ * replays a recorded arrival schedule). */
+bt_status bt_server_submit(bt_server* server, const bt_options* options, const float* xy, uint32_t n_points,
+                           const uint32_t* starts, uint32_t n_starts, uint32_t iterations, double arrival_s,
+                           uint64_t* id);
+/* The next request to finish or fail that was not returned before, in
+ * completion order; waits up to timeout_s (BT_ERR_TIMEOUT if none). */
+bt_status bt_server_next(bt_server* server, double timeout_s, bt_request_result* result);
+/* 12-byte {x, y, edge_id} records of a finished request, as bt_read_points. */
+bt_status bt_server_read_points(bt_server* server, uint64_t id, void* dst, size_t bytes);
+/* The finished request's context, for the other bt_read_* and bt_get_info
+ * calls until it is released; owned by the server (do not destroy or iterate
+ * it). NULL if the request has not finished or failed. */
+bt_ctx* bt_server_result(bt_server* server, uint64_t id);
+/* Gives a finished or failed request's memory back to the server. */
+bt_status bt_server_release(bt_server* server, uint64_t id);
+bt_status bt_server_stats_get(bt_server* server, bt_server_stats* stats);
 
 /* ---- Density blur without allocation ---- */
 

@@ -124,3 +124,30 @@ def test_batch_errors():
         batch.remove(3)
     batch.iterate(2)                       # an empty batch is a no-op
     assert batch.active() == 0
+
+
+def test_add_many_uploads_concurrently_and_matches_standalone():
+    jobs = mixed_jobs()
+    batch = bt.Batch()
+    added = batch.add_many([(o, w.xy, w.starts) for w, o in jobs])
+    assert [s for s, _ in added] == list(range(len(jobs)))
+    for (w, o), (slot, n) in zip(jobs, added):
+        assert batch.slot(slot).info().samples == n
+    batch.iterate(3)
+    for (w, o), (slot, _) in zip(jobs, added):
+        check_slot(batch, slot, standalone(w, o, 3))
+
+
+def test_add_many_is_all_or_nothing():
+    w = synthetic.small()
+    o = workload_options(w)
+    bad = w.starts.copy()
+    bad[-1] = w.xy.shape[0] + 5            # last start past the point count
+    batch = bt.Batch()
+    batch.add(o, w.xy, w.starts)
+    with pytest.raises(bt.BtError) as e:
+        batch.add_many([(o, w.xy, w.starts), (o, w.xy, bad)])
+    assert e.value.status == 3
+    assert batch.active() == 1
+    batch.iterate(1)
+    check_slot(batch, 0, standalone(w, o, 1))
