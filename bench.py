@@ -194,13 +194,6 @@ def profile_traffic():
     return None
 
 
-def scan_launches(n: int, tile: int = 1024) -> int:
-    """Launches of the cell-table scan (1024 cells per tile)."""
-    if n <= tile:
-        return 1
-    return 2 + scan_launches((n + tile - 1) // tile, tile)
-
-
 def workload(edges: int):
     from bundling_thingy_b200 import synthetic
 
@@ -338,7 +331,8 @@ def run_ours(args, ranks: Ranks):
     if ranks.rank == 0 and ranks.world == 1 and not args.no_cpu_baseline:
         cpu = cpu_sample(w, target_seconds=args.cpu_seconds)
 
-    per_iter = 1 + scan_launches(info.grid_width * info.fine_cells * info.grid_height * info.fine_cells) + 1 + 3
+    # mean, cell table, scatter, slot prefix (single-pass scans), blur H + V, normalise
+    per_iter = 7
     if (w.width * w.height) % 4:
         per_iter += 1
     line = {
@@ -349,7 +343,9 @@ def run_ours(args, ranks: Ranks):
         "config": {
             "workload": "large: 100k polylines (2-8 control points), 2048^2, spacing 1/1000, sigma 16 px, radius 16",
             "samples": n, "edges": w.edges, "grid": [w.width, w.height], "radius": w.radius, "sigma": w.sigma,
-            "search_cells_per_grid_cell": info.fine_cells, "iterations_per_job": ITERATIONS_PER_JOB,
+            "search_cells_per_grid_cell": {"x": info.fine_cells_x, "y": info.fine_cells,
+                                           "chosen": "at upload from the graph's density"},
+            "iterations_per_job": ITERATIONS_PER_JOB,
             "parallelism": f"replicas x{ranks.world}", "l2": "inputs larger than L2 (~330 MB working set per step)",
         },
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
@@ -393,21 +389,13 @@ def run_batched(args, ranks: Ranks):
         return bt.Options(width=j.width, height=j.height, neighbor_radius=j.radius, sample_spacing=j.spacing,
                           blur_sigma=j.sigma, device=device)
 
-    # Autotune the search-cell size once per (grid, radius) class.
-    t0 = time.perf_counter()
+    # Search-cell shapes are chosen per graph at upload from its density.
     firsts = {}
     for j in jobs:
         firsts.setdefault(key(j), j)
-    tuned = {}
-    for k, j in firsts.items():
-        o, ms = bt.autotune(options(j), j.xy, j.starts, 3)
-        tuned[k] = {"fine_cells": o.fine_cells, "ms_3_iterations": ms}
-    autotune_s = time.perf_counter() - t0
 
     def tuned_options(j):
-        o = options(j)
-        o.fine_cells = tuned[key(j)]["fine_cells"]
-        return o
+        return options(j)
 
     # Plain per-graph loop: one context per class, reused (Gpu::upload
     # releases the previous graph), upload + 10 x iterate + readback.
@@ -483,7 +471,7 @@ def run_batched(args, ranks: Ranks):
         "plain_seconds": {"iterations": t_iter, "total": plain_s},
         "batched_points_iter_per_s_device": ranks.sum(samples * iters) / (ranks.max(dev_ms) / 1e3),
         "iteration_speedup_vs_plain": t_iter / batch_iter_s,
-        "autotune": {"seconds": autotune_s, "classes": {f"{k[0]}px r{k[1]}": v for k, v in tuned.items()}},
+        "search_cells": "chosen per graph at upload from its density",
         "bit_exact_vs_plain": exact,
     }
     if ranks.rank == 0:
@@ -518,15 +506,7 @@ def run_served(args, ranks: Ranks):
     firsts = {}   # (grid, radius) class -> index of its first request
     for i, j in enumerate(jobs):
         firsts.setdefault(key(j), i)
-    tuned = {}
-    for k, i in firsts.items():
-        o, _ = bt.autotune(options(jobs[i]), jobs[i].xy, jobs[i].starts, 3)
-        tuned[k] = o.fine_cells
-    opts = []
-    for j in jobs:
-        o = options(j)
-        o.fine_cells = tuned[key(j)]
-        opts.append(o)
+    opts = [options(j) for j in jobs]   # search cells chosen per graph at upload
 
     host = {"buf": None}
 
@@ -639,7 +619,7 @@ def run_served(args, ranks: Ranks):
                                f"500-50k, grids 512/1024/2048, {iters} iterations, "
                                f"{args.budget_gb:g} GB admission budget",
                    "max_active": args.max_active, "max_step": args.max_step,
-                   "fine_cells": {f"{k[0]}px r{k[1]}": v for k, v in tuned.items()},
+                   "search_cells": "chosen per graph at upload from its density",
                    "parallelism": f"one arrival stream per rank x{ranks.world}"},
         "latency": pct(s_lat), "plain_latency": pct(p_lat),
         "plain_graphs_per_s": plain_gps, "speedup_vs_plain": served_gps / plain_gps,

@@ -61,7 +61,8 @@ class _Options(ctypes.Structure):
         ("evaluate_distortion", ctypes.c_uint32), ("device", ctypes.c_int32),
         ("sample_spacing", ctypes.c_float), ("blur_sigma", ctypes.c_float), ("blur_shrink", ctypes.c_float),
         ("fine_cells", ctypes.c_uint32), ("use_graphs", ctypes.c_uint32), ("timing", ctypes.c_uint32),
-        ("record_neighbors", ctypes.c_uint32), ("search_mode", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 6),
+        ("record_neighbors", ctypes.c_uint32), ("search_mode", ctypes.c_uint32), ("fine_cells_x", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32 * 5),
     ]
 
 
@@ -71,6 +72,7 @@ class _Info(ctypes.Structure):
         ("segments", ctypes.c_uint32), ("capacity", ctypes.c_uint32), ("iterations", ctypes.c_uint32),
         ("grid_width", ctypes.c_uint32), ("grid_height", ctypes.c_uint32), ("fine_cells", ctypes.c_uint32),
         ("density_passes", ctypes.c_uint32), ("device_bytes", ctypes.c_uint64), ("reserved_bytes", ctypes.c_uint64),
+        ("fine_cells_x", ctypes.c_uint32), ("reserved0", ctypes.c_uint32),
     ]
 
 
@@ -229,6 +231,7 @@ class Options:
     timing: bool = False
     record_neighbors: bool = False
     search_mode: int = 0     # 0: interior cells by prefix sums; 1: test every candidate (same results)
+    fine_cells_x: int = 0    # search cells per grid cell along x (0 = fine_cells)
 
     def _struct(self) -> _Options:
         o = _Options()
@@ -247,6 +250,7 @@ class Options:
         o.timing = int(bool(self.timing))
         o.record_neighbors = int(bool(self.record_neighbors))
         o.search_mode = int(self.search_mode)
+        o.fine_cells_x = self.fine_cells_x
         return o
 
     def resample_scale(self) -> tuple[float, float]:
@@ -313,6 +317,8 @@ class Info:
     density_passes: int
     device_bytes: int
     reserved_bytes: int
+    fine_cells_x: int
+    reserved0: int
 
 
 class Gpu:
@@ -443,8 +449,7 @@ class Gpu:
 
     def read_binning(self) -> tuple[np.ndarray, np.ndarray]:
         info = self.info()
-        k = info.fine_cells
-        cells = info.grid_width * k * info.grid_height * k
+        cells = info.grid_width * info.fine_cells_x * info.grid_height * info.fine_cells
         slots = np.zeros(info.samples, np.uint32)
         starts = np.zeros(cells + 1, np.uint32)
         self._ck(library().bt_read_binning(self._h, _p(slots, _u32p), slots.size, _p(starts, _u32p), starts.size))
@@ -489,7 +494,8 @@ def autotune(options: Options, xy: np.ndarray, starts: np.ndarray, iterations: i
     ms = np.zeros(1, np.float32)
     _check(library().bt_autotune(ctypes.byref(o), _p(xy, _f32p), xy.size // 2, _p(starts, _u32p), starts.size,
                                  iterations, ctypes.byref(tuned), _p(ms, _f32p)))
-    return dataclasses.replace(options, fine_cells=int(tuned.fine_cells)), float(ms[0])
+    return (dataclasses.replace(options, fine_cells=int(tuned.fine_cells), fine_cells_x=int(tuned.fine_cells_x)),
+            float(ms[0]))
 
 
 class _SlotView(Gpu):

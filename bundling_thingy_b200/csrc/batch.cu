@@ -32,8 +32,6 @@ namespace {
 
 constexpr uint32_t kSampleTile = 256;     // samples per mean / scatter tile
 constexpr uint32_t kTexelTile = 4096;     // texels per clear / normalise tile
-constexpr uint32_t kCellTile = static_cast<uint32_t>(scan_tile<LL3>());
-constexpr uint32_t kMaxCellTiles = kCellTile;   // one CTA scans a slot's tile sums
 constexpr uint32_t kTapsHorizon = 64;     // density passes of taps kept ahead
 
 struct BlurSlot {
@@ -53,12 +51,15 @@ struct SlotDesc {
     MeanArgs mean[2];        // by slot parity
     ScatterArgs scatter[2];  // by slot parity (writes the other order)
     const uint32_t* hist;
-    LL2* cellsum;
     uint32_t* cell_start;
-    LL2* cell_prefix;
-    LL3* tile_sums;          // cell_tiles + 1 entries
+    uint32_t* cell_sums;     // population sums per cell tile (from the mean), scanned in place (cell_tiles + 1)
+    const uint4* rec[2];     // records by slot parity
+    LL2* slot_prefix;
+    LL2* prefix_sums;        // position sums per prefix tile, scanned in place (prefix_tiles + 1)
     uint32_t cells;
     uint32_t cell_tiles;
+    uint32_t samples;
+    uint32_t prefix_tiles;
     BlurSlot blur;
 };
 
@@ -66,8 +67,11 @@ struct SlotState {
     uint32_t cur, pass, iterations, pad;
 };
 
-enum List : int { kSamples, kCells, kSlots, kBlurH, kBlurV, kTexels, kLists };
-enum Counter : int { cClear, cMean, cReduce, cSlotScan, cApply, cScatter, cBlurH, cBlurV, cNormalize, cCounters };
+enum List : int { kSamples, kCells, kSlots, kPrefix, kBlurH, kBlurV, kTexels, kLists };
+enum Counter : int {
+    cClear, cMean, cCellScan, cCellApply, cScatter, cPrefixReduce, cPrefixScan, cPrefixApply, cBlurH, cBlurV,
+    cNormalize, cCounters
+};
 
 struct BatchArgs {
     const SlotDesc* slots;
@@ -122,40 +126,72 @@ __global__ void __launch_bounds__(256, 5) batch_mean_kernel(BatchArgs b) {
     }
 }
 
-__global__ void __launch_bounds__(kScanBlock) batch_cell_reduce_kernel(BatchArgs b) {
+// Cell table: the population sums per tile (accumulated by the mean kernel)
+// scanned per slot, then each tile scanned from its offset into cell_start.
+// Each tile clears its sum after use, ready for the next iteration.
+__global__ void __launch_bounds__(kScanBlock) batch_cell_scan_kernel(BatchArgs b) {
     __shared__ uint32_t t_sh;
-    __shared__ ScanShared<LL3> sh;
+    __shared__ ScanShared<uint32_t> sh;
     uint32_t t;
-    while (next_tile(&b.counters[cReduce], b.counts[kCells], &t_sh, &t)) {
-        const uint2 tile = b.lists[kCells][t];
-        const SlotDesc& d = b.slots[tile.x];
-        const LL3 total = tile_reduce<LL3>(dev::CellAccSource{d.hist, d.cellsum},
-                                           static_cast<size_t>(tile.y) * kCellTile, d.cells, sh);
-        if (threadIdx.x == 0) d.tile_sums[tile.y] = total;
-    }
-}
-
-// Exclusive scan of each slot's tile sums, in place (one tile: <= 1024 sums).
-__global__ void __launch_bounds__(kScanBlock) batch_slot_scan_kernel(BatchArgs b) {
-    __shared__ uint32_t t_sh;
-    __shared__ ScanShared<LL3> sh;
-    uint32_t t;
-    while (next_tile(&b.counters[cSlotScan], b.counts[kSlots], &t_sh, &t)) {
+    while (next_tile(&b.counters[cCellScan], b.counts[kSlots], &t_sh, &t)) {
         const SlotDesc& d = b.slots[b.lists[kSlots][t].x];
-        tile_apply<LL3>(ArraySource<LL3>{d.tile_sums}, ArraySink<LL3>{d.tile_sums}, 0, d.cell_tiles, zero<LL3>(),
-                        sh);
+        block_scan_all<uint32_t>(ArraySource<uint32_t>{d.cell_sums}, ArraySink<uint32_t>{d.cell_sums}, d.cell_tiles,
+                                 sh);
     }
 }
 
 __global__ void __launch_bounds__(kScanBlock) batch_cell_apply_kernel(BatchArgs b) {
     __shared__ uint32_t t_sh;
-    __shared__ ScanShared<LL3> sh;
+    __shared__ ScanShared<uint32_t> sh;
     uint32_t t;
-    while (next_tile(&b.counters[cApply], b.counts[kCells], &t_sh, &t)) {
+    while (next_tile(&b.counters[cCellApply], b.counts[kCells], &t_sh, &t)) {
         const uint2 tile = b.lists[kCells][t];
         const SlotDesc& d = b.slots[tile.x];
-        tile_apply<LL3>(dev::CellAccSource{d.hist, d.cellsum}, dev::CellTableSink{d.cell_start, d.cell_prefix},
-                        static_cast<size_t>(tile.y) * kCellTile, d.cells, d.tile_sums[tile.y], sh);
+        const uint32_t offset = d.cell_sums[tile.y];
+        tile_apply<uint32_t>(ArraySource<uint32_t>{d.hist}, ArraySink<uint32_t>{d.cell_start},
+                             static_cast<size_t>(tile.y) * kCellTile, d.cells, offset, sh);
+        if (threadIdx.x == 0) {
+            d.cell_sums[tile.y] = 0u;
+            if (tile.y + 1 == d.cell_tiles) d.cell_sums[d.cell_tiles] = 0u;
+        }
+    }
+}
+
+// Slot prefix of the records the scatter just wrote (the other parity):
+// position sums per tile, scanned per slot, then each tile from its offset.
+__global__ void __launch_bounds__(kScanBlock) batch_prefix_reduce_kernel(BatchArgs b) {
+    __shared__ uint32_t t_sh;
+    __shared__ ScanShared<LL2> sh;
+    uint32_t t;
+    while (next_tile(&b.counters[cPrefixReduce], b.counts[kPrefix], &t_sh, &t)) {
+        const uint2 tile = b.lists[kPrefix][t];
+        const SlotDesc& d = b.slots[tile.x];
+        const LL2 total = tile_reduce<LL2>(dev::RecordQSource{d.rec[b.state[tile.x].cur ^ 1u]},
+                                           static_cast<size_t>(tile.y) * kPrefixTile, d.samples, sh);
+        if (threadIdx.x == 0) d.prefix_sums[tile.y] = total;
+    }
+}
+
+__global__ void __launch_bounds__(kScanBlock) batch_prefix_scan_kernel(BatchArgs b) {
+    __shared__ uint32_t t_sh;
+    __shared__ ScanShared<LL2> sh;
+    uint32_t t;
+    while (next_tile(&b.counters[cPrefixScan], b.counts[kSlots], &t_sh, &t)) {
+        const SlotDesc& d = b.slots[b.lists[kSlots][t].x];
+        block_scan_all<LL2>(ArraySource<LL2>{d.prefix_sums}, ArraySink<LL2>{d.prefix_sums}, d.prefix_tiles, sh);
+    }
+}
+
+__global__ void __launch_bounds__(kScanBlock) batch_prefix_apply_kernel(BatchArgs b) {
+    __shared__ uint32_t t_sh;
+    __shared__ ScanShared<LL2> sh;
+    uint32_t t;
+    while (next_tile(&b.counters[cPrefixApply], b.counts[kPrefix], &t_sh, &t)) {
+        const uint2 tile = b.lists[kPrefix][t];
+        const SlotDesc& d = b.slots[tile.x];
+        const LL2 offset = d.prefix_sums[tile.y];
+        tile_apply<LL2>(dev::RecordQSource{d.rec[b.state[tile.x].cur ^ 1u]}, ArraySink<LL2>{d.slot_prefix},
+                        static_cast<size_t>(tile.y) * kPrefixTile, d.samples, offset, sh);
     }
 }
 
@@ -244,7 +280,6 @@ struct Slot {
     DevBuf taps;             // Taps per density pass
     uint32_t taps_count = 0;
     uint32_t taps_first_pass = 0;   // taps[i] is pass i (tables start at pass 0)
-    DevBuf tile_sums;
 };
 
 }  // namespace
@@ -341,13 +376,13 @@ MeanArgs mean_args(bt_ctx* c, int src) {
     m.rec = c->sorted_rec[src].as<uint4>();
     m.tag = c->sorted_tag[src].as<uint32_t>();
     m.cell_start = c->cell_start.as<uint32_t>();
-    m.cell_prefix = c->cell_prefix.as<LL2>();
+    m.prefix = c->slot_prefix.as<LL2>();
     m.mode = static_cast<int>(c->opt.search_mode);
     m.out_xy = c->tmp_xy.as<float2>();
     m.out_tag = c->tmp_tag.as<uint32_t>();
     m.out_cell = c->tmp_cell.as<uint32_t>();
     m.hist = c->hist.as<uint32_t>();
-    m.cellsum = c->cellsum.as<LL2>();
+    m.hist_tiles = c->hist_tiles.as<uint32_t>();
     m.counts = c->accumulate ? c->counts.as<uint32_t>() : nullptr;
     m.neighbors = c->opt.record_neighbors ? c->neighbors.as<uint32_t>() : nullptr;
     m.n = c->samples;
@@ -388,10 +423,12 @@ void enqueue_batch_iteration(bt_batch* b) {
     cudaMemsetAsync(b->counters.p, 0, sizeof(uint32_t) * cCounters, b->stream);
     batch_clear_kernel<<<b->grid_blocks[cClear], 256, 0, b->stream>>>(a);
     batch_mean_kernel<<<b->grid_blocks[cMean], 256, 0, b->stream>>>(a);
-    batch_cell_reduce_kernel<<<b->grid_blocks[cReduce], kScanBlock, 0, b->stream>>>(a);
-    batch_slot_scan_kernel<<<b->grid_blocks[cSlotScan], kScanBlock, 0, b->stream>>>(a);
-    batch_cell_apply_kernel<<<b->grid_blocks[cApply], kScanBlock, 0, b->stream>>>(a);
+    batch_cell_scan_kernel<<<b->grid_blocks[cCellScan], kScanBlock, 0, b->stream>>>(a);
+    batch_cell_apply_kernel<<<b->grid_blocks[cCellApply], kScanBlock, 0, b->stream>>>(a);
     batch_scatter_kernel<<<b->grid_blocks[cScatter], 256, 0, b->stream>>>(a);
+    batch_prefix_reduce_kernel<<<b->grid_blocks[cPrefixReduce], kScanBlock, 0, b->stream>>>(a);
+    batch_prefix_scan_kernel<<<b->grid_blocks[cPrefixScan], kScanBlock, 0, b->stream>>>(a);
+    batch_prefix_apply_kernel<<<b->grid_blocks[cPrefixApply], kScanBlock, 0, b->stream>>>(a);
     batch_blur_h_kernel<<<b->grid_blocks[cBlurH], dev::kBlurThreads, b->blur_smem, b->stream>>>(a);
     batch_blur_v_kernel<<<b->grid_blocks[cBlurV], dev::kBlurThreads, b->blur_smem, b->stream>>>(a);
     batch_normalize_kernel<<<b->grid_blocks[cNormalize], 256, 0, b->stream>>>(a);
@@ -410,20 +447,27 @@ bt_status rebuild(bt_batch* b) {
         if (!s.active) continue;
         bt_ctx* c = s.ctx;
         if (bt_status st = fill_taps(b, s, std::max(b->max_pass, c->density_passes) + kTapsHorizon)) return st;
-        const uint32_t cell_tiles = static_cast<uint32_t>((c->cells + kCellTile - 1) / kCellTile);
-        if (bt_status st = bgrow(b, s.tile_sums, sizeof(LL3) * (cell_tiles + 1ull))) return st;
+        const uint32_t cell_tiles = static_cast<uint32_t>(scan_tiles<uint32_t>(c->cells));
+        const uint32_t prefix_tiles = static_cast<uint32_t>(scan_tiles<LL2>(c->samples));
+        // The population sums start from zero (each iteration's cell-table
+        // apply clears them after use).
+        BB_CUDA(b, cudaMemsetAsync(c->hist_tiles.p, 0, c->hist_tiles.bytes, b->stream));
         SlotDesc& d = descs[i];
         for (int p = 0; p < 2; ++p) {
             d.mean[p] = mean_args(c, p);
             d.scatter[p] = scatter_args(c, p, b->status.as<uint32_t>());
         }
         d.hist = c->hist.as<uint32_t>();
-        d.cellsum = c->cellsum.as<LL2>();
         d.cell_start = c->cell_start.as<uint32_t>();
-        d.cell_prefix = c->cell_prefix.as<LL2>();
-        d.tile_sums = s.tile_sums.as<LL3>();
+        d.cell_sums = c->hist_tiles.as<uint32_t>();
+        d.rec[0] = c->sorted_rec[0].as<uint4>();
+        d.rec[1] = c->sorted_rec[1].as<uint4>();
+        d.slot_prefix = c->slot_prefix.as<LL2>();
+        d.prefix_sums = c->prefix_tiles.as<LL2>();
         d.cells = static_cast<uint32_t>(c->cells);
         d.cell_tiles = cell_tiles;
+        d.samples = c->samples;
+        d.prefix_tiles = prefix_tiles;
         d.blur = BlurSlot{c->counts.as<uint32_t>(), c->himg.as<float>(), c->vimg.as<float>(), c->norm.as<float>(),
                           c->peak.as<uint32_t>(), c->map.w, c->map.h, c->texels, s.taps.as<Taps>(), s.taps_count,
                           c->accumulate ? 1u : 0u};
@@ -432,6 +476,7 @@ bt_status rebuild(bt_batch* b) {
         for (uint32_t t = 0; t < (c->samples + kSampleTile - 1) / kSampleTile; ++t)
             lists[kSamples].push_back(make_uint2(slot, t * kSampleTile));
         for (uint32_t t = 0; t < cell_tiles; ++t) lists[kCells].push_back(make_uint2(slot, t));
+        for (uint32_t t = 0; t < prefix_tiles; ++t) lists[kPrefix].push_back(make_uint2(slot, t));
         lists[kSlots].push_back(make_uint2(slot, 0u));
         if (c->accumulate) {
             const uint32_t hx = div_up(c->map.w, dev::kBlurSpan), hy = div_up(c->map.h, dev::kBlurLines);
@@ -504,8 +549,6 @@ bt_status batch_attach(bt_batch* b, bt_ctx* c, uint32_t* slot) {
     if (!c->uploaded || !c->has_grid)
         return bfail(b, BT_ERR_INVALID, "a batch slot needs an uploaded graph with a neighbour radius");
     if (c->device != b->device) return bfail(b, BT_ERR_INVALID, "the graph lives on another device");
-    if ((c->cells + kCellTile - 1) / kCellTile > kMaxCellTiles)
-        return bfail(b, BT_ERR_INVALID, "search grid too large for a batch slot (over 1M search cells)");
     // Reuse a free slot index, else append.
     uint32_t idx = 0;
     while (idx < b->slots.size() && b->slots[idx].active) ++idx;
@@ -570,10 +613,12 @@ bt_status bt_batch_create(int32_t device, bt_batch** out) {
     } ks[] = {
         {cClear, reinterpret_cast<const void*>(batch_clear_kernel), 256, 0},
         {cMean, reinterpret_cast<const void*>(batch_mean_kernel), 256, 0},
-        {cReduce, reinterpret_cast<const void*>(batch_cell_reduce_kernel), kScanBlock, 0},
-        {cSlotScan, reinterpret_cast<const void*>(batch_slot_scan_kernel), kScanBlock, 0},
-        {cApply, reinterpret_cast<const void*>(batch_cell_apply_kernel), kScanBlock, 0},
+        {cCellScan, reinterpret_cast<const void*>(batch_cell_scan_kernel), kScanBlock, 0},
+        {cCellApply, reinterpret_cast<const void*>(batch_cell_apply_kernel), kScanBlock, 0},
         {cScatter, reinterpret_cast<const void*>(batch_scatter_kernel), 256, 0},
+        {cPrefixReduce, reinterpret_cast<const void*>(batch_prefix_reduce_kernel), kScanBlock, 0},
+        {cPrefixScan, reinterpret_cast<const void*>(batch_prefix_scan_kernel), kScanBlock, 0},
+        {cPrefixApply, reinterpret_cast<const void*>(batch_prefix_apply_kernel), kScanBlock, 0},
         {cBlurH, reinterpret_cast<const void*>(batch_blur_h_kernel), dev::kBlurThreads, b->blur_smem},
         {cBlurV, reinterpret_cast<const void*>(batch_blur_v_kernel), dev::kBlurThreads, b->blur_smem},
         {cNormalize, reinterpret_cast<const void*>(batch_normalize_kernel), 256, 0},
@@ -607,7 +652,6 @@ void bt_batch_destroy(bt_batch* b) {
     for (Slot& s : b->slots) {
         bt_destroy(s.ctx);
         if (s.taps.p) cudaFree(s.taps.p);
-        if (s.tile_sums.p) cudaFree(s.tile_sums.p);
     }
     DevBuf* bufs[] = {&b->descs, &b->state, &b->counts, &b->counters, &b->status};
     for (DevBuf* x : bufs)
@@ -674,8 +718,7 @@ bt_status bt_batch_add_many(bt_batch* b, uint32_t count, const bt_options* optio
         if (bt_status s = upload_wait(ctxs[i])) return unwind(s, ctxs[i]->err);
     for (uint32_t i = 0; i < count; ++i) {
         if (bt_status s = upload_check(ctxs[i], &samples[i])) return unwind(s, ctxs[i]->err);
-        if ((ctxs[i]->cells + kCellTile - 1) / kCellTile > kMaxCellTiles)
-            return unwind(BT_ERR_INVALID, "search grid too large for a batch slot (over 1M search cells)");
+        if (bt_status s = upload_adapt(ctxs[i])) return unwind(s, ctxs[i]->err);
     }
     for (uint32_t i = 0; i < count; ++i) {
         batch_attach(b, ctxs[i], &slots[i]);   // cannot fail: every check above passed

@@ -60,16 +60,16 @@ __device__ __forceinline__ bool splat_index(float x, float y, const Map& m, uint
 }
 
 // Neighbour grid (neighbor_mean.rs:26-32, spatial_grid.wgsl:59-70) plus the
-// finer search cells: each grid cell side is split into k search cells.
+// finer search cells: each grid cell is split into kx x ky search cells.
 struct Grid {
     Map map;
     uint32_t radius;
     float rf;            // f32(radius)
     uint32_t gw, gh;     // grid cells: ceil(size / radius)
-    uint32_t k;          // search cells per grid cell side
-    float inv_s;         // f32(k) / f32(radius)
-    float s;             // search cell side in texels, f32(radius) / f32(k)
-    uint32_t fw, fh;     // search cells: gw * k, gh * k
+    uint32_t kx, ky;     // search cells per grid cell, along x and y
+    float inv_sx, inv_sy;// f32(k) / f32(radius)
+    float sx, sy;        // search cell sides in texels, f32(radius) / f32(k)
+    uint32_t fw, fh;     // search cells: gw * kx, gh * ky
     float tsx, tsy;      // texel_scale = f32(size - 1) * 0.5
     float r2;            // f32(radius) * f32(radius)
     float reachx, reachy;// f32(radius) + f32(size) * 2.4e-7 (neighbor_mean.wgsl:180-181)
@@ -91,17 +91,17 @@ __device__ __forceinline__ uint32_t grid_of(float t, float rf, uint32_t gsize) {
 
 // Search cell along one axis: the grid cell, then the sub-cell inside it, so
 // that search cell / k is exactly the reference's grid cell.
-__device__ __forceinline__ uint32_t search_of(float t, const Grid& g, uint32_t gsize) {
-    uint32_t c = grid_of(t, g.rf, gsize);
-    float rel = t - static_cast<float>(c) * g.rf;
-    uint32_t sub = u32_sat(rel * g.inv_s);
-    sub = sub < g.k - 1u ? sub : g.k - 1u;
-    return c * g.k + sub;
+__device__ __forceinline__ uint32_t search_of(float t, float rf, uint32_t gsize, uint32_t k, float inv_s) {
+    uint32_t c = grid_of(t, rf, gsize);
+    float rel = t - static_cast<float>(c) * rf;
+    uint32_t sub = u32_sat(rel * inv_s);
+    sub = sub < k - 1u ? sub : k - 1u;
+    return c * k + sub;
 }
 
 __device__ __forceinline__ uint32_t search_cell(float2 p, const Grid& g) {
-    uint32_t fx = search_of(texel_of(p.x, g.map.wm1), g, g.gw);
-    uint32_t fy = search_of(texel_of(p.y, g.map.hm1), g, g.gh);
+    uint32_t fx = search_of(texel_of(p.x, g.map.wm1), g.rf, g.gw, g.kx, g.inv_sx);
+    uint32_t fy = search_of(texel_of(p.y, g.map.hm1), g.rf, g.gh, g.ky, g.inv_sy);
     return fy * g.fw + fx;
 }
 

@@ -115,6 +115,9 @@ double sigma_for_pass(const bt_options& o, uint32_t pass) {
     return sigma;
 }
 
+// Search-cell shape chosen per graph (the options fix none).
+bool adaptive(const bt_ctx* c) { return c->opt.fine_cells == 0 && c->opt.fine_cells_x == 0; }
+
 bool constant_sigma(const bt_options& o) {
     return o.blur_sigma == 0.0f || o.blur_shrink == 0.0f || o.blur_shrink == 1.0f;
 }
@@ -123,6 +126,42 @@ bool constant_sigma(const bt_options& o) {
 uint64_t reference_grid_bytes(uint32_t w, uint32_t h, uint32_t r) {
     const uint64_t cells = static_cast<uint64_t>((w + r - 1) / r) * ((h + r - 1) / r);
     return cells * 8 + 8 + cells * 24 + 52;
+}
+
+void set_search_shape(bt::Grid& g, uint32_t ky, uint32_t kx) {
+    g.ky = ky;
+    g.kx = kx;
+    g.inv_sx = static_cast<float>(kx) / g.rf;
+    g.inv_sy = static_cast<float>(ky) / g.rf;
+    g.sx = g.rf / static_cast<float>(kx);
+    g.sy = g.rf / static_cast<float>(ky);
+    g.fw = g.gw * kx;
+    g.fh = g.gh * ky;
+}
+
+// Search-cell shape for a graph from the pairs of samples that share a grid
+// cell (sum of n (n - 1) over r x r cells). With rho the mean density around a
+// sample (samples per texel^2), a search costs about 2r / sy row lookups plus
+// rho 4r (sy + sx) exact tests per sample, and the cell table about 8 bytes a
+// cell per iteration: the best row height goes as 1 / sqrt(rho), and cells
+// about 8 times narrower than high pay for their table. The constants are
+// fitted to timings of whole iterations on B200 (after 8 iterations, over
+// graphs of 0.3 to 30 samples per texel^2 at upload, radius 4 to 16).
+void adaptive_shape(const bt_ctx* c, unsigned long long pairs, uint32_t* ky_out, uint32_t* kx_out) {
+    const bt::Grid& g = c->grid;
+    const double r = g.rf, n = static_cast<double>(c->samples);
+    const double rho = std::max(static_cast<double>(pairs) / (r * r * n), 1e-4);
+    const double sy = std::min(std::max(3.75 / std::sqrt(rho), 0.25), std::min(4.0, r));
+    uint32_t ky = static_cast<uint32_t>(std::min(std::max(std::lround(r / sy), 1L), 4096L));
+    uint32_t kx = std::min(8u * ky, 4096u);
+    // At most 32 Mi search cells (8 bytes each per iteration) and 8 per sample.
+    const uint64_t grid_cells = static_cast<uint64_t>(g.gw) * g.gh;
+    const uint64_t cap = std::min<uint64_t>(32ull << 20, std::max<uint64_t>(grid_cells, 8ull * c->samples));
+    if (grid_cells * ky * kx > cap) kx = static_cast<uint32_t>(std::max<uint64_t>(ky, cap / (grid_cells * ky)));
+    if (grid_cells * ky * kx > cap)
+        ky = kx = static_cast<uint32_t>(std::max(1.0, std::floor(std::sqrt(static_cast<double>(cap) / grid_cells))));
+    *ky_out = ky;
+    *kx_out = kx;
 }
 
 // Stage timing (GpuTimings, src/profiling.rs:35-136).
@@ -190,12 +229,13 @@ bt_status enqueue_density(bt_ctx* c, uint32_t pass) {
     return BT_OK;
 }
 
-// Cell table of the search-cell populations and sums, then the scatter into
-// slot order `dst`.
-void enqueue_binning(bt_ctx* c, int dst) {
+// Cell table of the search-cell populations (their tile sums accumulated by
+// the mean kernel when tiles_ready), the scatter into slot order `dst`, and
+// the slot prefix.
+void enqueue_binning(bt_ctx* c, int dst, bool tiles_ready) {
     stage_begin(c, "graph.grid_scan");
-    bt::launch_cell_table(c->hist.as<uint32_t>(), c->cellsum.as<bt::LL2>(), c->cells, c->cell_start.as<uint32_t>(),
-                          c->cell_prefix.as<bt::LL2>(), c->table_scratch.as<bt::LL3>(), c->stream);
+    bt::launch_cell_table(c->hist.as<uint32_t>(), c->cells, c->cell_start.as<uint32_t>(),
+                          c->hist_tiles.as<uint32_t>(), tiles_ready, c->stream);
     stage_end(c);
     stage_begin(c, "graph.grid_scatter");
     bt::ScatterArgs s{};
@@ -211,6 +251,10 @@ void enqueue_binning(bt_ctx* c, int dst) {
     s.status = c->status.as<uint32_t>();
     bt::launch_scatter(s, c->stream);
     stage_end(c);
+    stage_begin(c, "graph.slot_prefix");
+    bt::launch_slot_prefix(c->sorted_rec[dst].as<uint4>(), c->samples, c->slot_prefix.as<bt::LL2>(),
+                           c->prefix_tiles.as<bt::LL2>(), c->stream);
+    stage_end(c);
 }
 
 // One Gpu::iterate (gpu.rs:527-553) starting from slot order `src`.
@@ -219,25 +263,26 @@ bt_status enqueue_iteration(bt_ctx* c, int src, uint32_t pass) {
         cudaMemsetAsync(c->counts.p, 0, c->texels * sizeof(uint32_t), c->stream);
         cudaMemsetAsync(c->peak.p, 0, sizeof(uint32_t), c->stream);
     }
+    cudaMemsetAsync(c->hist_tiles.p, 0, c->hist_tiles.bytes, c->stream);
     stage_begin(c, "graph.neighbor_mean");
     bt::MeanArgs m{};
     m.rec = c->sorted_rec[src].as<uint4>();
     m.tag = c->sorted_tag[src].as<uint32_t>();
     m.cell_start = c->cell_start.as<uint32_t>();
-    m.cell_prefix = c->cell_prefix.as<bt::LL2>();
+    m.prefix = c->slot_prefix.as<bt::LL2>();
     m.mode = static_cast<int>(c->opt.search_mode);
     m.out_xy = c->tmp_xy.as<float2>();
     m.out_tag = c->tmp_tag.as<uint32_t>();
     m.out_cell = c->tmp_cell.as<uint32_t>();
     m.hist = c->hist.as<uint32_t>();
-    m.cellsum = c->cellsum.as<bt::LL2>();
+    m.hist_tiles = c->hist_tiles.as<uint32_t>();
     m.counts = c->accumulate ? c->counts.as<uint32_t>() : nullptr;
     m.neighbors = c->opt.record_neighbors ? c->neighbors.as<uint32_t>() : nullptr;
     m.n = c->samples;
     m.g = c->grid;
     bt::launch_neighbor_mean(m, c->stream);
     stage_end(c);
-    enqueue_binning(c, src ^ 1);
+    enqueue_binning(c, src ^ 1, true);
     if (c->accumulate) return enqueue_density(c, pass);
     return BT_OK;
 }
@@ -257,7 +302,8 @@ bt_status validate_options(const bt_options* o, bt_ctx* c) {
         return fail(c, BT_ERR_INVALID, "invalid sample spacing");
     if (o->sample_spacing > 0.0f && !std::isfinite(0.5 / static_cast<double>(o->sample_spacing)))
         return fail(c, BT_ERR_INVALID, "invalid sample spacing");
-    if (o->neighbor_radius > 0 && o->fine_cells > 4096) return fail(c, BT_ERR_INVALID, "fine_cells too large");
+    if (o->neighbor_radius > 0 && (o->fine_cells > 4096 || o->fine_cells_x > 4096))
+        return fail(c, BT_ERR_INVALID, "fine_cells too large");
     if (o->search_mode > 1) return fail(c, BT_ERR_INVALID, "unknown search_mode");
     const uint64_t grid = o->neighbor_radius ? reference_grid_bytes(o->width, o->height, o->neighbor_radius) : 0;
     const uint64_t staging = o->evaluate_distortion ? kDistortionStagingBytes : 0;
@@ -303,8 +349,8 @@ void bt_destroy(bt_ctx* c) {
     DevBuf* bufs[] = {&c->cp, &c->starts, &c->packed, &c->offsets, &c->scan64, &c->edges, &c->paths, &c->totals,
                       &c->status, &c->edge_ids, &c->segments, &c->tmp_xy, &c->tmp_tag, &c->tmp_cell,
                       &c->neighbors, &c->baseline, &c->current, &c->sorted_rec[0], &c->sorted_rec[1],
-                      &c->cellsum, &c->cell_prefix, &c->sorted_tag[0], &c->sorted_tag[1], &c->hist,
-                      &c->cell_start, &c->table_scratch, &c->counts, &c->himg, &c->vimg, &c->norm, &c->peak,
+                      &c->slot_prefix, &c->prefix_tiles, &c->sorted_tag[0], &c->sorted_tag[1], &c->hist,
+                      &c->cell_start, &c->hist_tiles, &c->counts, &c->himg, &c->vimg, &c->norm, &c->peak,
                       &c->records, &c->integrals};
     for (DevBuf* b : bufs) release(*b);
     if (c->account) c->account->used -= c->device_bytes;
@@ -370,13 +416,10 @@ bt_status bt::create_context(const bt_options* options, bt::MemAccount* account,
         g.rf = static_cast<float>(r);
         g.gw = (W + r - 1) / r;
         g.gh = (H + r - 1) / r;
-        // Search cells of about two texels by default (the fastest side on the
-        // large workload among 1, 2, 4 and 8 texels).
-        g.k = options->fine_cells ? options->fine_cells : std::max(1u, r / 2u);
-        g.inv_s = static_cast<float>(g.k) / g.rf;
-        g.s = g.rf / static_cast<float>(g.k);
-        g.fw = g.gw * g.k;
-        g.fh = g.gh * g.k;
+        // Square search cells of about two texels until the first upload picks
+        // a shape for the graph's density (unless the options fix one).
+        const uint32_t ky = options->fine_cells ? options->fine_cells : std::max(1u, r / 2u);
+        set_search_shape(g, ky, options->fine_cells_x ? options->fine_cells_x : ky);
         g.tsx = static_cast<float>(W - 1u) * 0.5f;
         g.tsy = static_cast<float>(H - 1u) * 0.5f;
         g.r2 = g.rf * g.rf;
@@ -388,12 +431,7 @@ bt_status bt::create_context(const bt_options* options, bt::MemAccount* account,
         c->grid_bytes_ref = reference_grid_bytes(W, H, r);
         if (bt_status s = ensure(c, c->hist, c->cells * 4)) return bail(s);
         if (bt_status s = ensure(c, c->cell_start, (c->cells + 1) * 4)) return bail(s);
-        if (bt_status s = ensure(c, c->cellsum, c->cells * sizeof(bt::LL2))) return bail(s);
-        if (bt_status s = ensure(c, c->cell_prefix, (c->cells + 1) * sizeof(bt::LL2))) return bail(s);
-        if (bt_status s = ensure(c, c->table_scratch, bt::cell_table_scratch(c->cells) * sizeof(bt::LL3)))
-            return bail(s);
-        if ((e = cudaMemsetAsync(c->cellsum.p, 0, c->cells * sizeof(bt::LL2), c->stream)) != cudaSuccess)
-            return bail(cuda_fail(c, e, "cudaMemset"));
+        if (bt_status s = ensure(c, c->hist_tiles, 4 * (bt::scan_tiles<uint32_t>(c->cells) + 1))) return bail(s);
         if ((e = cudaMemsetAsync(c->hist.p, 0, c->cells * 4, c->stream)) != cudaSuccess)
             return bail(cuda_fail(c, e, "cudaMemset"));
     }
@@ -523,6 +561,8 @@ bt_status bt::upload_finish(bt_ctx* c) {
             if (bt_status s = ensure(c, c->sorted_rec[b], 16ull * N)) return s;
             if (bt_status s = ensure(c, c->sorted_tag[b], 4ull * N)) return s;
         }
+        if (bt_status s = ensure(c, c->slot_prefix, 16ull * (N + 1ull))) return s;
+        if (bt_status s = ensure(c, c->prefix_tiles, 16 * (bt::scan_tiles<bt::LL2>(N) + 1))) return s;
         if (c->opt.record_neighbors)
             if (bt_status s = ensure(c, c->neighbors, 4ull * N)) return s;
     }
@@ -536,7 +576,6 @@ bt_status bt::upload_finish(bt_ctx* c) {
                                c->paths.as<bt::PathRec>(), c->stream);
     if (c->has_grid) {
         BT_CUDA(c, cudaMemsetAsync(c->hist.p, 0, c->cells * 4, c->stream));
-        BT_CUDA(c, cudaMemsetAsync(c->cellsum.p, 0, c->cells * sizeof(bt::LL2), c->stream));
     }
     if (c->accumulate) {
         BT_CUDA(c, cudaMemsetAsync(c->counts.p, 0, c->texels * 4, c->stream));
@@ -559,10 +598,11 @@ bt_status bt::upload_finish(bt_ctx* c) {
     ea.tag = c->tmp_tag.as<uint32_t>();
     ea.cell = c->tmp_cell.as<uint32_t>();
     ea.hist = c->hist.as<uint32_t>();
-    ea.cellsum = c->cellsum.as<bt::LL2>();
     ea.status = c->status.as<uint32_t>();
     bt::launch_resample_emit(ea, c->stream);
     stage_end(c);
+    if (c->has_grid && adaptive(c))
+        bt::launch_grid_pairs(c->hist.as<uint32_t>(), c->grid, c->totals.as<unsigned long long>() + 2, c->stream);
     c->samples = N;
     c->n_paths = E;
     c->drawn = static_cast<uint32_t>(drawn);
@@ -573,10 +613,39 @@ bt_status bt::upload_finish(bt_ctx* c) {
         c->density_passes = 1;
     }
     if (c->has_grid) {
-        enqueue_binning(c, 0);
+        enqueue_binning(c, 0, false);
         c->cur = 0;
     }
     BT_CUDA(c, cudaMemcpyAsync(c->h_status, c->status.p, 4, cudaMemcpyDeviceToHost, c->stream));
+    BT_CUDA(c, cudaMemcpyAsync(c->h_totals + 2, c->totals.as<unsigned long long>() + 2, 8, cudaMemcpyDeviceToHost,
+                               c->stream));
+    return BT_OK;
+}
+
+bt_status bt::upload_adapt(bt_ctx* c) {
+    if (!c->has_grid || !adaptive(c) || c->samples == 0) return BT_OK;
+    uint32_t ky = 0, kx = 0;
+    adaptive_shape(c, c->h_totals[2], &ky, &kx);
+    if (ky == c->grid.ky && kx == c->grid.kx) return BT_OK;
+    bt::Grid g = c->grid;
+    set_search_shape(g, ky, kx);
+    const size_t cells = static_cast<size_t>(g.fw) * g.fh;
+    // Allocations first: when one is refused (a memory budget), the graph
+    // keeps the shape it was binned with. New memory is not zero and the
+    // scatter left the rest of the populations zero, so all of it is cleared.
+    const bool room = ensure(c, c->hist, cells * 4) == BT_OK && ensure(c, c->cell_start, (cells + 1) * 4) == BT_OK &&
+                      ensure(c, c->hist_tiles, 4 * (bt::scan_tiles<uint32_t>(cells) + 1)) == BT_OK;
+    BT_CUDA(c, cudaMemsetAsync(c->hist.p, 0, c->hist.bytes, c->stream));
+    if (!room) return BT_OK;
+    c->grid = g;
+    c->cells = cells;
+    stage_begin(c, "graph.rebin");
+    bt::launch_rebin(c->sorted_rec[c->cur].as<uint4>(), c->sorted_tag[c->cur].as<uint32_t>(), c->samples, c->grid,
+                     c->tmp_xy.as<float2>(), c->tmp_tag.as<uint32_t>(), c->tmp_cell.as<uint32_t>(),
+                     c->hist.as<uint32_t>(), c->stream);
+    stage_end(c);
+    enqueue_binning(c, c->cur ^ 1, false);
+    c->cur ^= 1;
     return BT_OK;
 }
 
@@ -621,7 +690,8 @@ bt_status bt_upload(bt_ctx* c, const float* xy, uint32_t n_points, const uint32_
     if (bt_status s = wait(c)) return s;
     if (bt_status s = bt::upload_finish(c)) return s;
     if (bt_status s = wait(c)) return s;
-    return bt::upload_check(c, out_samples);
+    if (bt_status s = bt::upload_check(c, out_samples)) return s;
+    return bt::upload_adapt(c);
 }
 
 bt_status bt_upload_graph(bt_ctx* c, const bt_graph* g, uint32_t* out_samples) {
@@ -717,14 +787,22 @@ bt_status bt_autotune(const bt_options* options, const float* xy, uint32_t n_poi
     if (best_ms) *best_ms = 0.0f;
     const uint32_t r = options->neighbor_radius;
     if (r == 0 || iterations == 0) return BT_OK;
-    std::vector<uint32_t> candidates;
-    for (uint32_t k : {std::max(1u, r / 4u), std::max(1u, r / 2u), r, 2u * r})
-        if (k <= 4096 && std::find(candidates.begin(), candidates.end(), k) == candidates.end())
-            candidates.push_back(k);
+    // Search rows of 4, 2, 1 and 1/2 texels; cells as wide as high, or 2 or 4
+    // times narrower (a thinner boundary band for dense neighbourhoods).
+    std::vector<std::pair<uint32_t, uint32_t>> candidates;   // (ky, kx)
+    const uint64_t grid_cells = static_cast<uint64_t>((options->width + r - 1) / r) * ((options->height + r - 1) / r);
+    for (uint32_t ky : {std::max(1u, r / 4u), std::max(1u, r / 2u), r, 2u * r})
+        for (uint32_t m : {1u, 2u, 4u}) {
+            const uint32_t kx = ky * m;
+            const std::pair<uint32_t, uint32_t> kk{ky, kx};
+            if (kx > 4096 || grid_cells * ky * kx > (32ull << 20)) continue;
+            if (std::find(candidates.begin(), candidates.end(), kk) == candidates.end()) candidates.push_back(kk);
+        }
     float best = -1.0f;
-    for (uint32_t k : candidates) {
+    for (const auto& kk : candidates) {
         bt_options o = *options;
-        o.fine_cells = k;
+        o.fine_cells = kk.first;
+        o.fine_cells_x = kk.second;
         o.timing = 0;
         o.use_graphs = 1;
         bt_ctx* c = nullptr;
@@ -762,7 +840,8 @@ bt_status bt_get_info(bt_ctx* c, bt_info* info) {
     info->iterations = c->iterations;
     info->grid_width = c->has_grid ? c->grid.gw : 0;
     info->grid_height = c->has_grid ? c->grid.gh : 0;
-    info->fine_cells = c->has_grid ? c->grid.k : 0;
+    info->fine_cells = c->has_grid ? c->grid.ky : 0;
+    info->fine_cells_x = c->has_grid ? c->grid.kx : 0;
     info->density_passes = c->density_passes;
     info->device_bytes = c->device_bytes;
     info->reserved_bytes = c->reserved_bytes;

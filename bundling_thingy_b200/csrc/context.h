@@ -58,6 +58,10 @@ bt_status create_context(const bt_options* options, MemAccount* account, bt_ctx*
 bt_status upload_begin(bt_ctx* c, const float* xy, uint32_t n_points, const uint32_t* starts, uint32_t n_starts);
 bt_status upload_finish(bt_ctx* c);
 bt_status upload_check(bt_ctx* c, uint32_t* out_samples);
+// After the check: re-bins the graph under a search-cell shape chosen for
+// its density when the options leave the shape open (asynchronous; a refused
+// allocation keeps the current shape).
+bt_status upload_adapt(bt_ctx* c);
 bt_status upload_wait(bt_ctx* c);
 
 // Unsort the current positions into 12-byte records on the context's stream
@@ -94,7 +98,7 @@ struct bt_ctx {
     bt::DevBuf cp, starts, packed, offsets, scan64, edges, paths, totals, status;
     bt::DevBuf edge_ids, segments, tmp_xy, tmp_tag, tmp_cell, neighbors, baseline, current;
     bt::DevBuf sorted_rec[2], sorted_tag[2];
-    bt::DevBuf hist, cellsum, cell_start, cell_prefix, table_scratch;
+    bt::DevBuf hist, cell_start, hist_tiles, slot_prefix, prefix_tiles;
     bt::DevBuf counts, himg, vimg, norm, peak;
     bt::DevBuf records, integrals;
     unsigned long long* h_totals = nullptr;   // pinned

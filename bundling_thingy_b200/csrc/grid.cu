@@ -13,21 +13,25 @@
 //   p' = p + f32(f64(sum_q Q(q) - |N| Q(p)) / (f64(|N|) * 2^30)).
 //
 // B200 layout: samples live in slot order as 16-byte records
-// {x, y, Q(x) + 2^30, Q(y) + 2^30}, sorted by search cell (each grid cell side
-// split into k search cells, search cells row-major over the whole map), so a
-// row of search cells [a, b] is one contiguous slot range. A cell table (one
-// scan over the search cells) gives each cell's first slot and the sum of the
-// biased fixed-point positions of all earlier slots, which turns any such
-// range into one subtraction. Per search row, a thread takes the cells that
-// lie entirely inside its circle (by conservative bounds, with a margin far
-// above every f32 rounding involved) from the table — the role of the
-// reference's fully-contained cell summaries (neighbor_mean.wgsl:40-59) — and
-// tests only the samples of the boundary cells, exactly. The kernel writes the
-// new position in the same slot order (coalesced), and the new search cell's
-// population and position sum (warp-aggregated; this fuses count_cells of the
+// {x, y, Q(x) + 2^30, Q(y) + 2^30}, sorted by search cell (each grid cell split
+// into kx x ky search cells, search cells row-major over the whole map), so a
+// row of search cells [a, b] is one contiguous slot range. The cell table (a
+// scan of the search-cell populations) gives each cell's first slot, and the
+// slot prefix (a scan of the records) the sum of the biased fixed-point
+// positions of all earlier slots, which turns any such range into one
+// subtraction. Per search row, a thread takes the cells that lie entirely
+// inside its circle (by conservative bounds, with a margin far above every f32
+// rounding involved) from the prefix — the role of the reference's
+// fully-contained cell summaries (neighbor_mean.wgsl:40-59) — and tests only
+// the samples of the boundary cells, exactly. Flat search cells (kx > ky) cut
+// the boundary band: its area per circle is about 4 r (sy + sx) texels. The
+// kernel writes the new position in the same slot order (coalesced), the new
+// search cell's population (warp-aggregated; this fuses count_cells of the
 // next iteration), and its density splat. The scatter then moves the samples
 // into the next slot order, counting the populations back down to zero.
 // The per-sample bodies live in grid_dev.cuh (shared with batch.cu).
+#include <algorithm>
+
 #include "grid_dev.cuh"
 
 namespace bt {
@@ -79,6 +83,45 @@ __global__ void grid_cells_kernel(const uint4* rec, const uint32_t* tag, uint32_
     out[tag[s] & ~kMovableBit] = cy * g.gw + cx;
 }
 
+__global__ void __launch_bounds__(256) grid_pairs_kernel(const uint32_t* hist, Grid g, unsigned long long* out) {
+    __shared__ unsigned long long warp_sums[8];
+    const uint32_t cells = g.gw * g.gh;
+    unsigned long long acc = 0;
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < cells; c += gridDim.x * blockDim.x) {
+        const uint32_t gx = c % g.gw, gy = c / g.gw;
+        unsigned long long n = 0;
+        for (uint32_t sy = 0; sy < g.ky; ++sy) {
+            const uint32_t* row = hist + static_cast<size_t>(gy * g.ky + sy) * g.fw + static_cast<size_t>(gx) * g.kx;
+            for (uint32_t sx = 0; sx < g.kx; ++sx) n += row[sx];
+        }
+        acc += n * (n ? n - 1 : 0);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xFFFFFFFFu, acc, o);
+    if ((threadIdx.x & 31) == 0) warp_sums[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long total = 0;
+        for (int w = 0; w < 8; ++w) total += warp_sums[w];
+        atomicAdd(out, total);
+    }
+}
+
+__global__ void __launch_bounds__(256) rebin_kernel(const uint4* rec, const uint32_t* tag, uint32_t n, Grid g,
+                                                    float2* xy, uint32_t* out_tag, uint32_t* cell, uint32_t* hist) {
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = s < n;
+    const uint4 r = valid ? rec[s] : make_uint4(0u, 0u, 0u, 0u);
+    const float2 p = make_float2(__uint_as_float(r.x), __uint_as_float(r.y));
+    const uint32_t c = valid ? search_cell(p, g) : 0xFFFFFFFFu;
+    const unsigned peers = __match_any_sync(0xFFFFFFFFu, c);
+    if (!valid) return;
+    if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&hist[c], static_cast<uint32_t>(__popc(peers)));
+    xy[s] = p;
+    out_tag[s] = tag[s];
+    cell[s] = c;
+}
+
 __global__ void positions_kernel(const uint4* rec, const uint32_t* tag, uint32_t n, float2* out) {
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n) return;
@@ -98,13 +141,27 @@ void launch_scatter(const ScatterArgs& a, cudaStream_t s) {
     scatter_kernel<<<div_up(a.n, 256), 256, 0, s>>>(a);
 }
 
-size_t cell_table_scratch(size_t cells) { return scan_scratch_elems<LL3>(cells); }
-int cell_table_launches(size_t cells) { return scan_launch_count<LL3>(cells); }
+void launch_cell_table(const uint32_t* hist, size_t cells, uint32_t* cell_start, uint32_t* hist_tiles,
+                       bool tiles_ready, cudaStream_t s) {
+    if (!tiles_ready) reduce_tiles<uint32_t>(ArraySource<uint32_t>{hist}, cells, hist_tiles, s);
+    exclusive_scan_presummed<uint32_t>(ArraySource<uint32_t>{hist}, ArraySink<uint32_t>{cell_start}, cells,
+                                       hist_tiles, s);
+}
 
-void launch_cell_table(const uint32_t* hist, LL2* cellsum, size_t cells, uint32_t* cell_start, LL2* cell_prefix,
-                       LL3* scratch, cudaStream_t s) {
-    exclusive_scan_with<LL3>(dev::CellAccSource{hist, cellsum}, dev::CellTableSink{cell_start, cell_prefix}, cells,
-                             scratch, s);
+void launch_slot_prefix(const uint4* rec, uint32_t n, LL2* prefix, LL2* prefix_tiles, cudaStream_t s) {
+    reduce_tiles<LL2>(dev::RecordQSource{rec}, n, prefix_tiles, s);
+    exclusive_scan_presummed<LL2>(dev::RecordQSource{rec}, ArraySink<LL2>{prefix}, n, prefix_tiles, s);
+}
+
+void launch_grid_pairs(const uint32_t* hist, const Grid& g, unsigned long long* out, cudaStream_t s) {
+    const uint32_t cells = g.gw * g.gh;
+    grid_pairs_kernel<<<std::min(div_up(cells, 256), 1184u), 256, 0, s>>>(hist, g, out);
+}
+
+void launch_rebin(const uint4* rec, const uint32_t* tag, uint32_t n, const Grid& g, float2* xy, uint32_t* out_tag,
+                  uint32_t* cell, uint32_t* hist, cudaStream_t s) {
+    if (n == 0) return;
+    rebin_kernel<<<div_up(n, 256), 256, 0, s>>>(rec, tag, n, g, xy, out_tag, cell, hist);
 }
 
 void launch_unsort_records(const uint4* rec, const uint32_t* tag, const uint32_t* edge_ids, uint32_t n,

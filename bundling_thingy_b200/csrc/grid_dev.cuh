@@ -59,28 +59,28 @@ __device__ __forceinline__ void mean_sample(const MeanArgs& a, uint32_t i) {
         // Reach box in grid cells (neighbor_mean.wgsl:180-185), in search cells.
         const uint32_t cx0 = grid_of(tx - g.reachx, g.rf, g.gw), cx1 = grid_of(tx + g.reachx, g.rf, g.gw);
         const uint32_t cy0 = grid_of(ty - g.reachy, g.rf, g.gh), cy1 = grid_of(ty + g.reachy, g.rf, g.gh);
-        const int fx_min = static_cast<int>(cx0 * g.k), fx_max = static_cast<int>(cx1 * g.k + g.k - 1u);
-        const int fy_min = static_cast<int>(cy0 * g.k), fy_max = static_cast<int>(cy1 * g.k + g.k - 1u);
+        const int fx_min = static_cast<int>(cx0 * g.kx), fx_max = static_cast<int>(cx1 * g.kx + g.kx - 1u);
+        const int fy_min = static_cast<int>(cy0 * g.ky), fy_max = static_cast<int>(cy1 * g.ky + g.ky - 1u);
         // Candidate circle r + m; certain circle r - m (texels).
         const float R = g.rf + g.margin;
         const float Rin = g.rf - g.margin;
-        const int fy_lo = max(fy_min, floor_cell(ty - R, g.inv_s));
-        const int fy_hi = min(fy_max, floor_cell(ty + R, g.inv_s));
+        const int fy_lo = max(fy_min, floor_cell(ty - R, g.inv_sy));
+        const int fy_hi = min(fy_max, floor_cell(ty + R, g.inv_sy));
         const bool interior = a.mode == kSearchInterior;
         const int fw = static_cast<int>(g.fw), fh = static_cast<int>(g.fh);
         const float2 neg_p = make_float2(-p.x, -p.y);
         const float2 ts = make_float2(g.tsx, g.tsy);
         Acc acc{0ull, 0ull, 0u};
         for (int fy = fy_lo; fy <= fy_hi; ++fy) {
-            const float ylo = static_cast<float>(fy) * g.s;
-            const float yhi = ylo + g.s;
+            const float ylo = static_cast<float>(fy) * g.sy;
+            const float yhi = ylo + g.sy;
             const float near = fmaxf(fmaxf(ylo - ty, ty - yhi), 0.0f);
             const float dn = fmaxf(near - g.margin, 0.0f);
             if (dn > R) continue;
             // f32 rounding of R^2 - dn^2 is below 5e-7 R^2; widen by that.
             const float hout = sqrt_approx(fmaxf(R * R - dn * dn + 5e-7f * R * R, 0.0f)) * 1.000001f + g.margin;
-            const int bx0 = max(fx_min, floor_cell(tx - hout, g.inv_s));
-            const int bx1 = min(fx_max, floor_cell(tx + hout, g.inv_s));
+            const int bx0 = max(fx_min, floor_cell(tx - hout, g.inv_sx));
+            const int bx1 = min(fx_max, floor_cell(tx + hout, g.inv_sx));
             if (bx0 > bx1) continue;
             const uint32_t row = static_cast<uint32_t>(fy) * g.fw;
             const uint32_t s0 = a.cell_start[row + bx0];
@@ -94,15 +94,15 @@ __device__ __forceinline__ void mean_sample(const MeanArgs& a, uint32_t i) {
                     const float h2 = Rin * Rin - far * far - 5e-7f * Rin * Rin;
                     const float hin = sqrt_approx(fmaxf(h2, 0.0f)) * 0.999999f - g.margin;
                     if (hin > 0.0f) {
-                        ix0 = max(ceil_cell(tx - hin, g.inv_s), max(bx0, 1));
-                        ix1 = min(floor_cell(tx + hin, g.inv_s) - 1, min(bx1, fw - 2));
+                        ix0 = max(ceil_cell(tx - hin, g.inv_sx), max(bx0, 1));
+                        ix1 = min(floor_cell(tx + hin, g.inv_sx) - 1, min(bx1, fw - 2));
                     }
                 }
             }
             if (ix0 <= ix1) {
                 const uint32_t s1 = a.cell_start[row + ix0];
                 const uint32_t s2 = a.cell_start[row + ix1 + 1];
-                const LL2 lo = a.cell_prefix[row + ix0], hi = a.cell_prefix[row + ix1 + 1];
+                const LL2 lo = a.prefix[s1], hi = a.prefix[s2];
                 acc.sx += static_cast<unsigned long long>(hi.x - lo.x);
                 acc.sy += static_cast<unsigned long long>(hi.y - lo.y);
                 acc.count += s2 - s1;
@@ -120,22 +120,14 @@ __device__ __forceinline__ void mean_sample(const MeanArgs& a, uint32_t i) {
         np.x = p.x + static_cast<float>(static_cast<double>(dx) / den);
         np.y = p.y + static_cast<float>(static_cast<double>(dy) / den);
     }
-    // The next grid: search cell, population and biased position sum. Lanes
-    // of a warp that land in one cell (neighbours in slot order mostly do)
-    // add their counts and sums once.
+    // The next grid: search cell and population. Lanes of a warp that land
+    // in one cell (neighbours in slot order mostly do) add their count once.
     const uint32_t c = valid ? search_cell(np, g) : 0xFFFFFFFFu;
     const unsigned peers = __match_any_sync(0xFFFFFFFFu, c);
     if (!valid) return;
-    const uint32_t qx = biased_fixed(np.x), qy = biased_fixed(np.y);
-    // Group sums in 16-bit halves so each 32-bit reduction cannot overflow.
-    const uint32_t xl = __reduce_add_sync(peers, qx & 0xFFFFu), xh = __reduce_add_sync(peers, qx >> 16);
-    const uint32_t yl = __reduce_add_sync(peers, qy & 0xFFFFu), yh = __reduce_add_sync(peers, qy >> 16);
     if ((threadIdx.x & 31) == __ffs(peers) - 1) {
         atomicAdd(&a.hist[c], static_cast<uint32_t>(__popc(peers)));
-        atomicAdd(reinterpret_cast<unsigned long long*>(&a.cellsum[c].x),
-                  (static_cast<unsigned long long>(xh) << 16) + xl);
-        atomicAdd(reinterpret_cast<unsigned long long*>(&a.cellsum[c].y),
-                  (static_cast<unsigned long long>(yh) << 16) + yl);
+        if (a.hist_tiles) atomicAdd(&a.hist_tiles[c / kCellTile], static_cast<uint32_t>(__popc(peers)));
     }
     a.out_xy[i] = np;
     a.out_tag[i] = tag;
@@ -156,50 +148,36 @@ __device__ __forceinline__ void scatter_sample(const ScatterArgs& a, uint32_t i)
     // Lanes of one warp that share a cell (neighbours in slot order mostly do)
     // take one reservation and consecutive slots, so their writes coalesce.
     const unsigned peers = __match_any_sync(0xFFFFFFFFu, c);
-    if (!valid) return;
     // Cell ids and populations are consistent by construction; a failed
     // upload can leave stale entries, which are skipped and flagged.
-    if (c >= a.cells) {
-        atomicOr(a.status, 8u);
-        return;
-    }
+    bool ok = valid && c < a.cells;
+    if (valid && !ok) atomicOr(a.status, 8u);
     const int lane = threadIdx.x & 31;
     const int leader = __ffs(peers) - 1;
     const uint32_t group = __popc(peers);
     const uint32_t rank = __popc(peers & ((1u << lane) - 1u));
     uint32_t top = 0;
-    if (lane == leader) top = atomicSub(&a.hist[c], group);
-    top = __shfl_sync(peers, top, leader);
-    const uint32_t slot = a.cell_start[c] + (top - group) + rank;
-    if (top < group || slot >= a.n) {
+    if (ok && lane == leader) top = atomicSub(&a.hist[c], group);
+    top = __shfl_sync(0xFFFFFFFFu, top, leader);
+    const uint32_t slot = ok ? a.cell_start[c] + (top - group) + rank : 0u;
+    if (ok && (top < group || slot >= a.n)) {
         atomicOr(a.status, 8u);
-        return;
+        ok = false;
     }
+    if (!ok) return;
     const float2 p = a.xy[i];
     a.out_rec[slot] = make_uint4(__float_as_uint(p.x), __float_as_uint(p.y), biased_fixed(p.x), biased_fixed(p.y));
     a.out_tag[slot] = a.tag[i];
 }
 
-// Cell-table scan input: a cell's population and position sums; the sums are
-// cleared after their last read so the next iteration accumulates from zero.
-struct CellAccSource {
-    const uint32_t* hist;
-    LL2* cellsum;
-    __device__ __forceinline__ LL3 read(size_t j) const {
-        const LL2 s = cellsum[j];
-        return LL3{static_cast<long long>(hist[j]), s.x, s.y};
+// Slot-prefix scan input: the biased fixed-point position of a record.
+struct RecordQSource {
+    const uint4* rec;
+    __device__ __forceinline__ LL2 read(size_t j) const {
+        const uint4 r = rec[j];
+        return LL2{static_cast<long long>(r.z), static_cast<long long>(r.w)};
     }
-    __device__ __forceinline__ void consume(size_t j) const { cellsum[j] = LL2{0, 0}; }
-};
-
-// Cell-table scan output: first slot and prefix sums of each search cell.
-struct CellTableSink {
-    uint32_t* cell_start;
-    LL2* cell_prefix;
-    __device__ __forceinline__ void store(size_t j, LL3 v) const {
-        cell_start[j] = static_cast<uint32_t>(v.c);
-        cell_prefix[j] = LL2{v.x, v.y};
-    }
+    __device__ __forceinline__ void consume(size_t) const {}
 };
 
 }  // namespace dev

@@ -51,7 +51,6 @@ struct ResampleEmitArgs {
     uint32_t* tag;           // sample index | movable bit, sample order
     uint32_t* cell;          // search cell of each sample
     uint32_t* hist;          // search-cell populations
-    LL2* cellsum;            // search-cell sums of the biased fixed-point positions
     uint32_t* status;        // bit 1: count/emit mismatch
 };
 void launch_resample_emit(const ResampleEmitArgs& a, cudaStream_t s);
@@ -78,12 +77,6 @@ __device__ __forceinline__ uint32_t biased_fixed(float v) {
     return static_cast<uint32_t>(__float2int_rn(v * kFixedScale)) + kFixedBias;
 }
 
-// Adds a sample's biased fixed-point position to its cell's sums.
-__device__ __forceinline__ void add_cell_sum(LL2* cellsum, uint32_t c, uint32_t qx, uint32_t qy) {
-    atomicAdd(reinterpret_cast<unsigned long long*>(&cellsum[c].x), static_cast<unsigned long long>(qx));
-    atomicAdd(reinterpret_cast<unsigned long long*>(&cellsum[c].y), static_cast<unsigned long long>(qy));
-}
-
 enum SearchMode : int {
     kSearchInterior = 0,   // interior search cells from the prefix sums, boundary ring tested exactly
     kSearchScanAll = 1,    // every sample of the candidate search cells tested exactly
@@ -93,12 +86,12 @@ struct MeanArgs {
     const uint4* rec;        // slot order (sorted by search cell)
     const uint32_t* tag;     // sample index | movable bit, slot order
     const uint32_t* cell_start;   // cell table: first slot of each search cell (cells + 1)
-    const LL2* cell_prefix;  // cell table: sum of the biased positions of all earlier slots (cells + 1)
+    const LL2* prefix;       // sum of the biased positions of all earlier slots (n + 1)
     float2* out_xy;          // new positions, same slot order
     uint32_t* out_tag;
     uint32_t* out_cell;      // search cell of the new position
     uint32_t* hist;          // populations of the next grid
-    LL2* cellsum;            // biased position sums of the next grid
+    uint32_t* hist_tiles;    // their sums per cell-table tile (zero before the launch)
     uint32_t* counts;        // density splat (nullptr = off)
     uint32_t* neighbors;     // |N(p)| per slot (nullptr = off)
     uint32_t n;
@@ -107,12 +100,32 @@ struct MeanArgs {
 };
 void launch_neighbor_mean(const MeanArgs& a, cudaStream_t s);
 
-// Cell table of the next slot order from the populations and sums (the sums
-// are cleared for reuse; the populations stay for the scatter's count-down).
-void launch_cell_table(const uint32_t* hist, LL2* cellsum, size_t cells, uint32_t* cell_start, LL2* cell_prefix,
-                       LL3* scratch, cudaStream_t s);
-size_t cell_table_scratch(size_t cells);
-int cell_table_launches(size_t cells);
+// Tiles of the cell table (search cells) and of the slot prefix (slots).
+constexpr uint32_t kCellTile = static_cast<uint32_t>(scan_tile<uint32_t>());
+constexpr uint32_t kPrefixTile = static_cast<uint32_t>(scan_tile<LL2>());
+
+// Cell table of the next slot order: the first slot of each search cell, an
+// exclusive scan of the populations (which stay for the scatter's count-down).
+// hist_tiles (scan_tiles(cells) + 1 entries) holds the populations' sums per
+// tile when tiles_ready (the mean kernel accumulates them), else they are
+// reduced here.
+void launch_cell_table(const uint32_t* hist, size_t cells, uint32_t* cell_start, uint32_t* hist_tiles,
+                       bool tiles_ready, cudaStream_t s);
+
+// Pairs of samples sharing a grid cell (r x r texels): sum over grid cells of
+// n (n - 1), from the search-cell populations; added to *out.
+void launch_grid_pairs(const uint32_t* hist, const Grid& g, unsigned long long* out, cudaStream_t s);
+
+// Re-bins slot-order records under another search-cell shape: positions,
+// tags and new search cells in slot order (the scatter's input) and the new
+// populations (hist must be zero).
+void launch_rebin(const uint4* rec, const uint32_t* tag, uint32_t n, const Grid& g, float2* xy, uint32_t* out_tag,
+                  uint32_t* cell, uint32_t* hist, cudaStream_t s);
+
+// Slot prefix of the scattered records: prefix[j] = sum over slots < j of the
+// biased fixed-point positions (n + 1 entries); prefix_tiles (scan_tiles(n) +
+// 1 entries) is its scratch.
+void launch_slot_prefix(const uint4* rec, uint32_t n, LL2* prefix, LL2* prefix_tiles, cudaStream_t s);
 
 struct ScatterArgs {
     const float2* xy;

@@ -132,7 +132,6 @@ __device__ __forceinline__ void write_sample(const EmitKernelArgs& k, const Path
         a.tag[index] = index | (movable ? kMovableBit : 0u);
         a.cell[index] = c;
         atomicAdd(&a.hist[c], 1u);
-        add_cell_sum(a.cellsum, c, biased_fixed(s.x), biased_fixed(s.y));
     }
 }
 

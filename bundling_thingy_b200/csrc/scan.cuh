@@ -31,20 +31,6 @@ __host__ __device__ __forceinline__ LL2& operator+=(LL2& a, LL2 b) {
     return a;
 }
 
-// Count and fixed-point sums of a search cell; its exclusive prefix over the
-// cells is the cell table {first slot, sum of the positions before it}.
-struct LL3 {
-    long long c, x, y;
-};
-__host__ __device__ __forceinline__ LL3 operator+(LL3 a, LL3 b) { return LL3{a.c + b.c, a.x + b.x, a.y + b.y}; }
-__host__ __device__ __forceinline__ LL3 operator-(LL3 a, LL3 b) { return LL3{a.c - b.c, a.x - b.x, a.y - b.y}; }
-__host__ __device__ __forceinline__ LL3& operator+=(LL3& a, LL3 b) {
-    a.c += b.c;
-    a.x += b.x;
-    a.y += b.y;
-    return a;
-}
-
 template <typename T>
 __device__ __forceinline__ T zero() {
     return T(0);
@@ -52,10 +38,6 @@ __device__ __forceinline__ T zero() {
 template <>
 __device__ __forceinline__ LL2 zero<LL2>() {
     return LL2{0, 0};
-}
-template <>
-__device__ __forceinline__ LL3 zero<LL3>() {
-    return LL3{0, 0, 0};
 }
 
 template <typename T>
@@ -66,11 +48,6 @@ template <>
 __device__ __forceinline__ LL2 shfl_up<LL2>(LL2 v, int o) {
     return LL2{__shfl_up_sync(0xFFFFFFFFu, v.x, o), __shfl_up_sync(0xFFFFFFFFu, v.y, o)};
 }
-template <>
-__device__ __forceinline__ LL3 shfl_up<LL3>(LL3 v, int o) {
-    return LL3{__shfl_up_sync(0xFFFFFFFFu, v.c, o), __shfl_up_sync(0xFFFFFFFFu, v.x, o),
-               __shfl_up_sync(0xFFFFFFFFu, v.y, o)};
-}
 template <typename T>
 __device__ __forceinline__ T shfl_down(T v, int o) {
     return __shfl_down_sync(0xFFFFFFFFu, v, o);
@@ -79,16 +56,12 @@ template <>
 __device__ __forceinline__ LL2 shfl_down<LL2>(LL2 v, int o) {
     return LL2{__shfl_down_sync(0xFFFFFFFFu, v.x, o), __shfl_down_sync(0xFFFFFFFFu, v.y, o)};
 }
-template <>
-__device__ __forceinline__ LL3 shfl_down<LL3>(LL3 v, int o) {
-    return LL3{__shfl_down_sync(0xFFFFFFFFu, v.c, o), __shfl_down_sync(0xFFFFFFFFu, v.x, o),
-               __shfl_down_sync(0xFFFFFFFFu, v.y, o)};
-}
 
-// Items per thread: tiles of 2048 elements up to 16 bytes, 1024 above.
+// Items per thread: tiles of 4096 elements of 4 bytes, 2048 up to 16 bytes,
+// 1024 above.
 template <typename T>
 __host__ __device__ constexpr int scan_items() {
-    return sizeof(T) <= 16 ? 8 : 4;
+    return sizeof(T) <= 4 ? 16 : sizeof(T) <= 16 ? 8 : 4;
 }
 template <typename T>
 __host__ __device__ constexpr size_t scan_tile() {
@@ -157,10 +130,19 @@ __device__ __forceinline__ T block_exclusive(T v, T* warp_sums, T* total) {
     return prefix;
 }
 
-// Shared memory of one tile pass (padded to avoid bank conflicts).
+// Shared-memory index of tile element i: one element of padding per 128
+// bytes, so that both the striped stores (thread t, element k * 256 + t) and
+// the blocked loads (thread t, elements t * items ..) are free of bank
+// conflicts for 4- to 16-byte elements.
+template <typename T>
+__host__ __device__ constexpr int scan_pad(int i) {
+    return i + i / static_cast<int>(128 / sizeof(T));
+}
+
+// Shared memory of one tile pass.
 template <typename T>
 struct ScanShared {
-    T tile[scan_tile<T>() + scan_tile<T>() / 32];
+    T tile[scan_pad<T>(static_cast<int>(scan_tile<T>()))];
     T warp_sums[kScanBlock / 32 + 1];
 };
 
@@ -178,13 +160,14 @@ __device__ __forceinline__ T tile_reduce(const Source& in, size_t base, size_t n
 }
 
 // out[j] = offset + sum(in[base .. j)) for the tile at base; the tile that
-// reaches n also stores the total at n. Synchronises internally.
+// reaches n also stores the total at n. Returns offset + the tile's sum (to
+// every thread). Synchronises internally.
 template <typename T, typename Source, typename Sink>
-__device__ __forceinline__ void tile_apply(const Source& in, const Sink& out, size_t base, size_t n, T offset,
-                                           ScanShared<T>& sh) {
+__device__ __forceinline__ T tile_apply(const Source& in, const Sink& out, size_t base, size_t n, T offset,
+                                        ScanShared<T>& sh) {
     constexpr int kItems = scan_items<T>();
     constexpr int kTile = kScanBlock * kItems;
-    auto pad = [](int i) { return i + (i >> 5); };
+    auto pad = [](int i) { return scan_pad<T>(i); };
 #pragma unroll
     for (int i = 0; i < kItems; ++i) {
         int t = i * kScanBlock + threadIdx.x;
@@ -221,6 +204,19 @@ __device__ __forceinline__ void tile_apply(const Source& in, const Sink& out, si
     }
     if (threadIdx.x == 0 && base + kTile >= n) out.store(n, offset + block_total);
     __syncthreads();
+    return offset + block_total;
+}
+
+// Exclusive scan of in[0 .. n) by one block, tile after tile (out may alias
+// in: each tile is staged in shared memory before it is written).
+template <typename T, typename Source, typename Sink>
+__device__ __forceinline__ void block_scan_all(const Source& in, const Sink& out, size_t n, ScanShared<T>& sh) {
+    T carry = zero<T>();
+    size_t base = 0;
+    do {
+        carry = tile_apply<T>(in, out, base, n, carry, sh);
+        base += scan_tile<T>();
+    } while (base < n);
 }
 
 template <typename T, typename Source>
@@ -277,6 +273,40 @@ void exclusive_scan_with(Source in, Sink out, size_t n, T* scratch, cudaStream_t
 template <typename T>
 void exclusive_scan(const T* in, T* out, size_t n, T* scratch, cudaStream_t stream) {
     exclusive_scan_with<T>(ArraySource<T>{in}, ArraySink<T>{out}, n, scratch, stream);
+}
+
+// ---- Scans whose producer accumulated the tile sums ----
+//
+// A kernel that writes the scan's input can add each element to the sum of its
+// tile (scan_tile<T>() elements) as it goes; the scan is then one block over
+// the tile sums and one pass over the tiles, reading the data once.
+
+template <typename T>
+inline size_t scan_tiles(size_t n) {
+    const size_t t = (n + scan_tile<T>() - 1) / scan_tile<T>();
+    return t ? t : 1;
+}
+
+// Exclusive scan of the tile sums in place by one block (sums[count] = total).
+template <typename T>
+__global__ void __launch_bounds__(kScanBlock) tile_sums_scan_kernel(T* sums, size_t count) {
+    __shared__ ScanShared<T> sh;
+    block_scan_all<T>(ArraySource<T>{sums}, ArraySink<T>{sums}, count, sh);
+}
+
+// Exclusive scan of n elements given the sums of their tiles (scan_tiles(n)
+// + 1 entries, scanned in place); the sink receives n + 1 values.
+template <typename T, typename Source, typename Sink>
+void exclusive_scan_presummed(Source in, Sink out, size_t n, T* tile_sums, cudaStream_t stream) {
+    const size_t tiles = scan_tiles<T>(n);
+    tile_sums_scan_kernel<T><<<1, kScanBlock, 0, stream>>>(tile_sums, tiles);
+    scan_apply_kernel<T, Source, Sink><<<static_cast<unsigned>(tiles), kScanBlock, 0, stream>>>(in, n, tile_sums, out);
+}
+
+// The tile sums of n elements, for a producer that did not accumulate them.
+template <typename T, typename Source>
+void reduce_tiles(Source in, size_t n, T* tile_sums, cudaStream_t stream) {
+    scan_reduce_kernel<T, Source><<<static_cast<unsigned>(scan_tiles<T>(n)), kScanBlock, 0, stream>>>(in, n, tile_sums);
 }
 
 }  // namespace bt

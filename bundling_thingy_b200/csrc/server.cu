@@ -293,6 +293,7 @@ void finish_uploads(bt_server* s) {
         uint32_t samples = 0;
         bt_status st = bt::upload_wait(r->ctx);
         if (st == BT_OK) st = bt::upload_check(r->ctx, &samples);
+        if (st == BT_OK) st = bt::upload_adapt(r->ctx);
         if (st == BT_OK) st = bt::reserve_records(r->ctx);
         if (st == BT_OK && r->iterations == 0) {
             // Nothing to iterate: the upload is the result.

@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define BT_ABI_VERSION 1
+#define BT_ABI_VERSION 2
 
 typedef int32_t bt_status;
 enum {
@@ -59,13 +59,15 @@ typedef struct bt_options {
     float sample_spacing;           /* resample spacing as a fraction of the canvas; 0 = one texel */
     float blur_sigma;               /* Gaussian sigma in texels; 0 = the fixed sigma-6 table */
     float blur_shrink;              /* sigma factor per density pass; 0 or 1 = none */
-    uint32_t fine_cells;            /* neighbour-search cells per grid cell side; 0 = automatic */
+    uint32_t fine_cells;            /* neighbour-search cells per grid cell along y (and along x when
+                                       fine_cells_x is 0); 0 = automatic */
     uint32_t use_graphs;            /* capture the iteration in a CUDA graph (1 = on, default) */
     uint32_t timing;                /* record per-stage CUDA-event timings */
     uint32_t record_neighbors;      /* keep |N(p)| of the last iteration for bt_read_neighbors */
     uint32_t search_mode;           /* 0: interior search cells from prefix sums, boundary tested
                                        sample by sample; 1: every candidate tested (same results) */
-    uint32_t reserved[6];
+    uint32_t fine_cells_x;          /* neighbour-search cells per grid cell along x; 0 = fine_cells */
+    uint32_t reserved[5];
 } bt_options;
 
 typedef struct bt_info {
@@ -77,10 +79,12 @@ typedef struct bt_info {
     uint32_t iterations;      /* neighbour-mean iterations since upload */
     uint32_t grid_width;      /* neighbour grid cells (neighbor_mean.rs:26-32) */
     uint32_t grid_height;
-    uint32_t fine_cells;      /* search cells per grid cell side */
+    uint32_t fine_cells;      /* search cells per grid cell along y */
     uint32_t density_passes;  /* blur passes since upload */
     uint64_t device_bytes;    /* device memory held by the context */
     uint64_t reserved_bytes;  /* budget accounting of the reference (resampling.rs:394-395) */
+    uint32_t fine_cells_x;    /* search cells per grid cell along x */
+    uint32_t reserved0;
 } bt_info;
 
 typedef struct bt_ctx bt_ctx;
@@ -170,9 +174,11 @@ bt_status bt_stage_times(bt_ctx* ctx, const char** names, float* ms, uint32_t ca
 
 /* Autotuner (beyond the reference): times `iterations` iterations of this
  * graph (after one warm-up iteration, CUDA events on the context's stream)
- * for each candidate search-cell size — 1/4, 1/2, 1 and 2 search cells per
- * texel of radius — and writes the fastest options to *tuned (its time to
- * *best_ms when not NULL). Every candidate gives bit-identical results. */
+ * for each candidate search-cell shape — rows of 4, 2, 1 and 1/2 texels
+ * (fine_cells = r/4, r/2, r, 2r) with cells 1, 2 or 4 times narrower than
+ * high (fine_cells_x), at most 32 Mi search cells — and writes the fastest
+ * options to *tuned (its time to *best_ms when not NULL). Every candidate
+ * gives bit-identical results. */
 bt_status bt_autotune(const bt_options* options, const float* xy, uint32_t n_points, const uint32_t* starts,
                       uint32_t n_starts, uint32_t iterations, bt_options* tuned, float* best_ms);
 

@@ -28,7 +28,12 @@ def test_bindings_cover_the_header(lib):
 
 
 def test_abi_version(lib):
-    assert lib.bt_abi_version() == 1
+    header = open(HEADER).read()
+    version = int(re.search(r"#define BT_ABI_VERSION (\d+)", header).group(1))
+    assert lib.bt_abi_version() == version
+    # The ctypes mirrors keep the C layouts (no padding holes in either).
+    assert ctypes.sizeof(bt._Options) == 88
+    assert ctypes.sizeof(bt._Info) == 64
 
 
 def test_options_defaults_match_reference(lib):

@@ -33,6 +33,10 @@ def mixed_jobs():
         (small2, workload_options(small2, color_by=bt.COLOR_BY_EDGE_ID)),   # no density passes
         (small, workload_options(small, width=512, height=512, neighbor_radius=1, blur_sigma=3.0,
                                  blur_shrink=1.0, search_mode=1)),
+        # 8M flat search cells: the per-slot scan of the cell-table tile sums
+        # runs over more than one tile.
+        (small2, workload_options(small2, width=2048, height=2048, neighbor_radius=4, blur_sigma=4.0,
+                                  blur_shrink=1.0, fine_cells=4, fine_cells_x=8)),
     ]
 
 

@@ -151,10 +151,11 @@ def test_large_config_invariants_over_iterations():
     np.testing.assert_array_equal(runs[0], runs[1])
 
 
-@pytest.mark.parametrize("fine", [1, 3, 0])
-def test_search_cell_size_does_not_change_results(oracle, fine):
+@pytest.mark.parametrize("fine,fine_x", [(1, 0), (3, 0), (0, 0), (2, 8), (6, 24), (12, 12), (1, 5)])
+def test_search_cell_size_does_not_change_results(oracle, fine, fine_x):
+    # Square and flat search cells enumerate the same N(p).
     w = synthetic.small()
-    o = opts_for(w, neighbor_radius=6, fine_cells=fine)
+    o = opts_for(w, neighbor_radius=6, fine_cells=fine, fine_cells_x=fine_x)
     gpu, ora = pair(oracle, w.xy, w.starts, o)
     gpu.iterate(2)
     ora.iterate(2)
@@ -210,8 +211,8 @@ def test_grid_cells_and_binning(oracle):
     info = gpu.info()
     assert (info.grid_width, info.grid_height) == (gw, gh)
     slots, starts = gpu.read_binning()
-    k = info.fine_cells
-    fw = gw * k
+    ky, kx = info.fine_cells, info.fine_cells_x
+    fw = gw * kx
     assert starts[-1] == info.samples
     assert np.all(np.diff(starts.astype(np.int64)) >= 0)
     assert np.array_equal(np.sort(slots), np.arange(info.samples))
@@ -219,7 +220,7 @@ def test_grid_cells_and_binning(oracle):
     # cell's population equals the oracle's (compared as sets of samples).
     cell_of_slot = np.repeat(np.arange(starts.size - 1), np.diff(starts))
     fx, fy = cell_of_slot % fw, cell_of_slot // fw
-    coarse = (fy // k) * gw + (fx // k)
+    coarse = (fy // ky) * gw + (fx // kx)
     np.testing.assert_array_equal(coarse, cells[slots])
 
 
@@ -354,3 +355,27 @@ def test_stage_timings():
     assert {"graph.neighbor_mean", "graph.grid_scan", "graph.grid_scatter",
             "density.blur_vertical_and_maximum", "density.normalize"} <= set(it)
     assert all(v >= 0 for v in it.values())
+
+
+def test_autotune_returns_an_equivalent_shape(oracle):
+    w = synthetic.small()
+    tuned, ms = bt.autotune(opts_for(w), w.xy, w.starts, 2)
+    assert ms > 0
+    assert tuned.fine_cells >= 1 and tuned.fine_cells_x >= tuned.fine_cells
+    gpu, ora = pair(oracle, w.xy, w.starts, tuned)
+    gpu.iterate(2)
+    ora.iterate(2)
+    check_points(gpu, ora)
+
+
+def test_upload_picks_flat_search_cells_for_dense_graphs(oracle):
+    # The shape is chosen from the graph's density at upload; any shape
+    # enumerates the same neighbourhoods.
+    w = synthetic.mid()
+    gpu, ora = pair(oracle, w.xy, w.starts, opts_for(w))
+    info = gpu.info()
+    assert info.fine_cells_x > info.fine_cells >= 1
+    gpu.iterate(2)
+    ora.iterate(2)
+    check_points(gpu, ora)
+    check_density(gpu, ora)
