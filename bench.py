@@ -58,6 +58,9 @@ def parse_args():
     p.add_argument("--rate", type=float, default=200.0, help="served workload: mean arrivals per second")
     p.add_argument("--capacity-requests", type=int, default=300,
                    help="served workload: requests of the all-at-once capacity run (0 = skip)")
+    p.add_argument("--sustained-rate", type=float, default=40.0,
+                   help="served workload: a lower arrival rate both arms sustain, for latency (0 = skip)")
+    p.add_argument("--sustained-requests", type=int, default=200)
     p.add_argument("--max-active", type=int, default=32)
     p.add_argument("--max-step", type=int, default=1)
     p.add_argument("--budget-gb", type=float, default=120.0)
@@ -606,8 +609,23 @@ def run_served(args, ranks: Ranks):
         c_p = plain_run(at_once)
         capacity = {"requests": m, "served_graphs_per_s": ranks.sum(m / ranks.max(c_s[1])),
                     "plain_graphs_per_s": ranks.sum(m / ranks.max(c_p[1])),
-                    "served_peak_active": c_s[4]["peak_active"]}
+                    "served_peak_active": c_s[4]["peak_active"],
+                    "server": {k: c_s[4][k] for k in ("steps", "launch_s", "upload_s", "wait_s", "retire_s", "idle_s",
+                                                       "contexts_created", "create_s")}}
         capacity["speedup_vs_plain"] = capacity["served_graphs_per_s"] / capacity["plain_graphs_per_s"]
+
+    sustained = None
+    if args.sustained_rate > 0 and args.sustained_requests > 0:
+        m = min(args.sustained_requests, n)
+        sched = np.asarray(arrivals[:m]) * (args.rate / args.sustained_rate)   # same draws, slower clock
+        ranks.barrier()
+        u_s = served_run(sched)
+        ranks.barrier()
+        u_p = plain_run(sched)
+        sustained = {"rate": args.sustained_rate, "requests": m,
+                     "served_graphs_per_s": ranks.sum(m / ranks.max(u_s[1])),
+                     "plain_graphs_per_s": ranks.sum(m / ranks.max(u_p[1])),
+                     "latency": pct(u_s[0]), "plain_latency": pct(u_p[0])}
 
     served_gps = ranks.sum(n / ranks.max(s_span))
     plain_gps = ranks.sum(n / ranks.max(p_span))
@@ -624,9 +642,12 @@ def run_served(args, ranks: Ranks):
         "latency": pct(s_lat), "plain_latency": pct(p_lat),
         "plain_graphs_per_s": plain_gps, "speedup_vs_plain": served_gps / plain_gps,
         "served_points_iter_per_s": ranks.sum(s_samples * iters / s_span),
-        "server": {k: stats[k] for k in ("peak_active", "peak_device_bytes", "budget_waits", "evictions", "steps")},
+        "server": {k: stats[k] for k in ("peak_active", "peak_device_bytes", "budget_waits", "evictions", "steps",
+                                         "launch_s", "upload_s", "wait_s", "retire_s", "idle_s", "contexts_created",
+                                         "create_s")},
         "submit_seconds": submit_s, "arrivals_late": late,
         "capacity_all_at_once": capacity,
+        "sustained": sustained,
         "bit_exact_vs_plain": exact,
         "clocks": clock_info,
     }

@@ -98,7 +98,9 @@ class _ServerStats(ctypes.Structure):
         ("steps", ctypes.c_uint64), ("rebuilds", ctypes.c_uint64), ("budget_waits", ctypes.c_uint64),
         ("evictions", ctypes.c_uint64), ("queued", ctypes.c_uint32), ("active", ctypes.c_uint32),
         ("peak_active", ctypes.c_uint32), ("resident_results", ctypes.c_uint32), ("device_bytes", ctypes.c_uint64),
-        ("peak_device_bytes", ctypes.c_uint64),
+        ("peak_device_bytes", ctypes.c_uint64), ("launch_s", ctypes.c_double), ("upload_s", ctypes.c_double),
+        ("wait_s", ctypes.c_double), ("retire_s", ctypes.c_double), ("idle_s", ctypes.c_double),
+        ("contexts_created", ctypes.c_uint64), ("create_s", ctypes.c_double),
     ]
 
 

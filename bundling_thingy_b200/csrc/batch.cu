@@ -325,10 +325,11 @@ bt_status bcuda(bt_batch* b, cudaError_t e, const char* what) {
 bt_status bgrow(bt_batch* b, DevBuf& buf, size_t bytes) {
     if (bytes == 0) bytes = 16;
     if (buf.bytes >= bytes) return BT_OK;
-    if (buf.p) cudaFree(buf.p);
+    // Stream-ordered, like the contexts' buffers: no device-wide wait.
+    if (buf.p) cudaFreeAsync(buf.p, b->stream);
     buf.p = nullptr;
     buf.bytes = 0;
-    cudaError_t e = cudaMalloc(&buf.p, bytes);
+    cudaError_t e = cudaMallocAsync(&buf.p, bytes, b->stream);
     if (e != cudaSuccess) {
         cudaGetLastError();
         return bcuda(b, e, "device allocation");
@@ -366,7 +367,8 @@ bt_status fill_taps(bt_batch* b, Slot& s, uint32_t upto) {
     for (uint32_t i = 0; i < count; ++i)
         if (!make_blur_taps(sigma_for_pass(o, i), &taps[i])) return bfail(b, BT_ERR_INVALID, "invalid blur sigma");
     if (bt_status st = bgrow(b, s.taps, sizeof(Taps) * count)) return st;
-    BB_CUDA(b, cudaMemcpy(s.taps.p, taps.data(), sizeof(Taps) * count, cudaMemcpyHostToDevice));
+    // Stream-ordered like the allocation (the host copy is staged before the call returns).
+    BB_CUDA(b, cudaMemcpyAsync(s.taps.p, taps.data(), sizeof(Taps) * count, cudaMemcpyHostToDevice, b->stream));
     s.taps_count = count;
     return BT_OK;
 }
@@ -549,6 +551,12 @@ bt_status batch_attach(bt_batch* b, bt_ctx* c, uint32_t* slot) {
     if (!c->uploaded || !c->has_grid)
         return bfail(b, BT_ERR_INVALID, "a batch slot needs an uploaded graph with a neighbour radius");
     if (c->device != b->device) return bfail(b, BT_ERR_INVALID, "the graph lives on another device");
+    // The batch's next launches come after the work still queued on the
+    // context's stream (an upload's re-binning runs asynchronously).
+    cudaSetDevice(b->device);
+    cudaError_t e = cudaEventRecord(c->done, c->stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(b->stream, c->done, 0);
+    if (e != cudaSuccess) return bcuda(b, e, "stream ordering");
     // Reuse a free slot index, else append.
     uint32_t idx = 0;
     while (idx < b->slots.size() && b->slots[idx].active) ++idx;
@@ -562,6 +570,8 @@ bt_status batch_attach(bt_batch* b, bt_ctx* c, uint32_t* slot) {
     *slot = idx;
     return BT_OK;
 }
+
+cudaStream_t batch_stream(bt_batch* b) { return b->stream; }
 
 bt_ctx* batch_detach(bt_batch* b, uint32_t slot) {
     bt_ctx* c = nullptr;
@@ -651,13 +661,14 @@ void bt_batch_destroy(bt_batch* b) {
     if (b->graph) cudaGraphExecDestroy(b->graph);
     for (Slot& s : b->slots) {
         bt_destroy(s.ctx);
-        if (s.taps.p) cudaFree(s.taps.p);
+        if (s.taps.p) cudaFreeAsync(s.taps.p, b->stream);
     }
     DevBuf* bufs[] = {&b->descs, &b->state, &b->counts, &b->counters, &b->status};
     for (DevBuf* x : bufs)
-        if (x->p) cudaFree(x->p);
+        if (x->p) cudaFreeAsync(x->p, b->stream);
     for (DevBuf& x : b->lists)
-        if (x.p) cudaFree(x.p);
+        if (x.p) cudaFreeAsync(x.p, b->stream);
+    if (b->stream) cudaStreamSynchronize(b->stream);   // the frees above
     if (b->h_status) cudaFreeHost(b->h_status);
     if (b->done) cudaEventDestroy(b->done);
     if (b->t0) cudaEventDestroy(b->t0);

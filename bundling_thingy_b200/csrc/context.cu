@@ -61,13 +61,15 @@ bt_status ensure(bt_ctx* c, DevBuf& b, size_t bytes) {
                 return fail(c, BT_ERR_BUDGET, "device memory budget of the server is exhausted");
         } while (!c->account->used.compare_exchange_weak(used, used + growth));
     }
+    // Stream-ordered: neither the free nor the allocation waits for the rest
+    // of the device (a serving worker allocates while batches run).
     if (b.p) {
-        cudaFree(b.p);
+        cudaFreeAsync(b.p, c->stream);
         c->device_bytes -= b.bytes;
         b.p = nullptr;
         b.bytes = 0;
     }
-    cudaError_t e = cudaMalloc(&b.p, bytes);
+    cudaError_t e = cudaMallocAsync(&b.p, bytes, c->stream);
     if (e != cudaSuccess) {
         cudaGetLastError();
         if (c->account) c->account->used -= bytes;   // the old buffer is gone too
@@ -78,8 +80,8 @@ bt_status ensure(bt_ctx* c, DevBuf& b, size_t bytes) {
     return BT_OK;
 }
 
-void release(DevBuf& b) {
-    if (b.p) cudaFree(b.p);
+void release(DevBuf& b, cudaStream_t stream) {
+    if (b.p) cudaFreeAsync(b.p, stream);
     b.p = nullptr;
     b.bytes = 0;
 }
@@ -165,7 +167,7 @@ void adaptive_shape(const bt_ctx* c, unsigned long long pairs, uint32_t* ky_out,
 }
 
 // Stage timing (GpuTimings, src/profiling.rs:35-136).
-void stage_begin(bt_ctx* c, const char* name) {
+void stage_begin(bt_ctx* c, const char* name, cudaStream_t stream = nullptr) {
     if (!c->opt.timing) return;
     if (c->stage_used == c->stage_pool.size()) {
         StageRec r{name, nullptr, nullptr};
@@ -175,12 +177,12 @@ void stage_begin(bt_ctx* c, const char* name) {
     }
     StageRec& r = c->stage_pool[c->stage_used++];
     r.name = name;
-    cudaEventRecord(r.start, c->stream);
+    cudaEventRecord(r.start, stream ? stream : c->stream);
 }
 
-void stage_end(bt_ctx* c) {
+void stage_end(bt_ctx* c, cudaStream_t stream = nullptr) {
     if (!c->opt.timing || c->stage_used == 0) return;
-    cudaEventRecord(c->stage_pool[c->stage_used - 1].stop, c->stream);
+    cudaEventRecord(c->stage_pool[c->stage_used - 1].stop, stream ? stream : c->stream);
 }
 
 bt_status wait(bt_ctx* c) {
@@ -212,20 +214,20 @@ void drop_graphs(bt_ctx* c) {
     }
 }
 
-// Density::encode (density.rs:155-166) for density pass `pass`.
-bt_status enqueue_density(bt_ctx* c, uint32_t pass) {
+// Density::encode (density.rs:155-166) for density pass `pass`, on `stream`.
+bt_status enqueue_density(bt_ctx* c, uint32_t pass, cudaStream_t stream) {
     bt::Taps taps;
     if (!blur_taps(sigma_for_pass(c->opt, pass), &taps)) return fail(c, BT_ERR_INVALID, "invalid blur sigma");
-    stage_begin(c, "density.blur_horizontal");
-    bt::launch_blur_horizontal(c->counts.as<uint32_t>(), c->himg.as<float>(), c->map.w, c->map.h, taps, c->stream);
-    stage_end(c);
-    stage_begin(c, "density.blur_vertical_and_maximum");
+    stage_begin(c, "density.blur_horizontal", stream);
+    bt::launch_blur_horizontal(c->counts.as<uint32_t>(), c->himg.as<float>(), c->map.w, c->map.h, taps, stream);
+    stage_end(c, stream);
+    stage_begin(c, "density.blur_vertical_and_maximum", stream);
     bt::launch_blur_vertical(c->himg.as<float>(), c->vimg.as<float>(), c->map.w, c->map.h, taps,
-                             c->peak.as<uint32_t>(), c->stream);
-    stage_end(c);
-    stage_begin(c, "density.normalize");
-    bt::launch_normalize(c->vimg.as<float>(), c->peak.as<uint32_t>(), c->norm.as<float>(), c->texels, c->stream);
-    stage_end(c);
+                             c->peak.as<uint32_t>(), stream);
+    stage_end(c, stream);
+    stage_begin(c, "density.normalize", stream);
+    bt::launch_normalize(c->vimg.as<float>(), c->peak.as<uint32_t>(), c->norm.as<float>(), c->texels, stream);
+    stage_end(c, stream);
     return BT_OK;
 }
 
@@ -282,9 +284,20 @@ bt_status enqueue_iteration(bt_ctx* c, int src, uint32_t pass) {
     m.g = c->grid;
     bt::launch_neighbor_mean(m, c->stream);
     stage_end(c);
+    if (!c->accumulate) {
+        enqueue_binning(c, src ^ 1, true);
+        return BT_OK;
+    }
+    // The density passes read only the splat counts and the binning never
+    // touches the density images: the two branches run concurrently, joined
+    // before the next iteration clears the counts.
+    BT_CUDA(c, cudaEventRecord(c->fork, c->stream));
+    BT_CUDA(c, cudaStreamWaitEvent(c->side, c->fork, 0));
+    bt_status s = enqueue_density(c, pass, c->side);
+    BT_CUDA(c, cudaEventRecord(c->join, c->side));
     enqueue_binning(c, src ^ 1, true);
-    if (c->accumulate) return enqueue_density(c, pass);
-    return BT_OK;
+    BT_CUDA(c, cudaStreamWaitEvent(c->stream, c->join, 0));
+    return s;
 }
 
 bt_status validate_options(const bt_options* o, bt_ctx* c) {
@@ -345,6 +358,7 @@ bt_status bt_create(const bt_options* options, bt_ctx** out) { return bt::create
 void bt_destroy(bt_ctx* c) {
     if (!c) return;
     if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->side) cudaStreamSynchronize(c->side);
     drop_graphs(c);
     DevBuf* bufs[] = {&c->cp, &c->starts, &c->packed, &c->offsets, &c->scan64, &c->edges, &c->paths, &c->totals,
                       &c->status, &c->edge_ids, &c->segments, &c->tmp_xy, &c->tmp_tag, &c->tmp_cell,
@@ -352,7 +366,8 @@ void bt_destroy(bt_ctx* c) {
                       &c->slot_prefix, &c->prefix_tiles, &c->sorted_tag[0], &c->sorted_tag[1], &c->hist,
                       &c->cell_start, &c->hist_tiles, &c->counts, &c->himg, &c->vimg, &c->norm, &c->peak,
                       &c->records, &c->integrals};
-    for (DevBuf* b : bufs) release(*b);
+    for (DevBuf* b : bufs) release(*b, c->stream);
+    if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->account) c->account->used -= c->device_bytes;
     for (StageRec& r : c->stage_pool) {
         cudaEventDestroy(r.start);
@@ -363,6 +378,9 @@ void bt_destroy(bt_ctx* c) {
     if (c->done) cudaEventDestroy(c->done);
     if (c->t0) cudaEventDestroy(c->t0);
     if (c->t1) cudaEventDestroy(c->t1);
+    if (c->fork) cudaEventDestroy(c->fork);
+    if (c->join) cudaEventDestroy(c->join);
+    if (c->side) cudaStreamDestroy(c->side);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -386,8 +404,12 @@ bt_status bt::create_context(const bt_options* options, bt::MemAccount* account,
     cudaError_t e = cudaSetDevice(c->device);
     if (e != cudaSuccess) return bail(cuda_fail(c, e, "cudaSetDevice"));
     if ((e = bt::prepare_density_kernels()) != cudaSuccess) return bail(cuda_fail(c, e, "kernel attributes"));
-    if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess)
+    if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking)) != cudaSuccess)
         return bail(cuda_fail(c, e, "cudaStreamCreate"));
+    if ((e = cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&c->join, cudaEventDisableTiming)) != cudaSuccess)
+        return bail(cuda_fail(c, e, "cudaEventCreate"));
     if ((e = cudaEventCreateWithFlags(&c->done, cudaEventDisableTiming)) != cudaSuccess)
         return bail(cuda_fail(c, e, "cudaEventCreate"));
     if ((e = cudaMallocHost(&c->h_totals, 4 * sizeof(unsigned long long))) != cudaSuccess)
@@ -602,14 +624,15 @@ bt_status bt::upload_finish(bt_ctx* c) {
     bt::launch_resample_emit(ea, c->stream);
     stage_end(c);
     if (c->has_grid && adaptive(c))
-        bt::launch_grid_pairs(c->hist.as<uint32_t>(), c->grid, c->totals.as<unsigned long long>() + 2, c->stream);
+        bt::launch_grid_pairs(c->hist.as<uint32_t>(), c->grid, c->cell_start.as<uint32_t>(),   // scratch until binned
+                              c->totals.as<unsigned long long>() + 2, c->stream);
     c->samples = N;
     c->n_paths = E;
     c->drawn = static_cast<uint32_t>(drawn);
     if (c->opt.evaluate_distortion)
         BT_CUDA(c, cudaMemcpyAsync(c->baseline.p, c->tmp_xy.p, 8ull * N, cudaMemcpyDeviceToDevice, c->stream));
     if (c->accumulate) {
-        if (bt_status s = enqueue_density(c, 0)) return s;
+        if (bt_status s = enqueue_density(c, 0, c->stream)) return s;
         c->density_passes = 1;
     }
     if (c->has_grid) {

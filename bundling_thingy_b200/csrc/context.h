@@ -74,6 +74,8 @@ bt_status copy_records(bt_ctx* c, void* dst, size_t bytes);
 // and take it back without destroying it; detach waits for the batch.
 bt_status batch_attach(bt_batch* b, bt_ctx* c, uint32_t* slot);
 bt_ctx* batch_detach(bt_batch* b, uint32_t slot);
+// The stream the batch's steps run on.
+cudaStream_t batch_stream(bt_batch* b);
 }  // namespace bt
 
 struct bt_graph {
@@ -84,6 +86,8 @@ struct bt_ctx {
     bt_options opt{};
     int device = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t side = nullptr;              // density passes, overlapped with the binning
+    cudaEvent_t fork = nullptr, join = nullptr;
     cudaEvent_t done = nullptr;
     cudaEvent_t t0 = nullptr, t1 = nullptr;
     std::string err;

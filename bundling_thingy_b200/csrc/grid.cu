@@ -83,17 +83,25 @@ __global__ void grid_cells_kernel(const uint4* rec, const uint32_t* tag, uint32_
     out[tag[s] & ~kMovableBit] = cy * g.gw + cx;
 }
 
-__global__ void __launch_bounds__(256) grid_pairs_kernel(const uint32_t* hist, Grid g, unsigned long long* out) {
+// Populations of the reference's grid cells (r x r) from the search-cell
+// populations; counts is zero before the launch.
+__global__ void __launch_bounds__(256) grid_counts_kernel(const uint32_t* hist, Grid g, uint32_t* counts) {
+    const size_t cells = static_cast<size_t>(g.fw) * g.fh;
+    for (size_t c = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; c < cells;
+         c += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        const uint32_t n = hist[c];
+        if (n == 0) continue;
+        const uint32_t fx = static_cast<uint32_t>(c % g.fw), fy = static_cast<uint32_t>(c / g.fw);
+        atomicAdd(&counts[(fy / g.ky) * g.gw + fx / g.kx], n);
+    }
+}
+
+__global__ void __launch_bounds__(256) grid_pairs_kernel(const uint32_t* counts, uint32_t n_cells,
+                                                         unsigned long long* out) {
     __shared__ unsigned long long warp_sums[8];
-    const uint32_t cells = g.gw * g.gh;
     unsigned long long acc = 0;
-    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < cells; c += gridDim.x * blockDim.x) {
-        const uint32_t gx = c % g.gw, gy = c / g.gw;
-        unsigned long long n = 0;
-        for (uint32_t sy = 0; sy < g.ky; ++sy) {
-            const uint32_t* row = hist + static_cast<size_t>(gy * g.ky + sy) * g.fw + static_cast<size_t>(gx) * g.kx;
-            for (uint32_t sx = 0; sx < g.kx; ++sx) n += row[sx];
-        }
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < n_cells; c += gridDim.x * blockDim.x) {
+        const unsigned long long n = counts[c];
         acc += n * (n ? n - 1 : 0);
     }
 #pragma unroll
@@ -153,9 +161,14 @@ void launch_slot_prefix(const uint4* rec, uint32_t n, LL2* prefix, LL2* prefix_t
     exclusive_scan_presummed<LL2>(dev::RecordQSource{rec}, ArraySink<LL2>{prefix}, n, prefix_tiles, s);
 }
 
-void launch_grid_pairs(const uint32_t* hist, const Grid& g, unsigned long long* out, cudaStream_t s) {
-    const uint32_t cells = g.gw * g.gh;
-    grid_pairs_kernel<<<std::min(div_up(cells, 256), 1184u), 256, 0, s>>>(hist, g, out);
+void launch_grid_pairs(const uint32_t* hist, const Grid& g, uint32_t* scratch, unsigned long long* out,
+                       cudaStream_t s) {
+    const uint32_t grid_cells = g.gw * g.gh;
+    const size_t cells = static_cast<size_t>(g.fw) * g.fh;
+    cudaMemsetAsync(scratch, 0, 4ull * grid_cells, s);
+    grid_counts_kernel<<<static_cast<unsigned>(std::min<size_t>((cells + 255) / 256, 148 * 16)), 256, 0, s>>>(
+        hist, g, scratch);
+    grid_pairs_kernel<<<std::min(div_up(grid_cells, 256), 1184u), 256, 0, s>>>(scratch, grid_cells, out);
 }
 
 void launch_rebin(const uint4* rec, const uint32_t* tag, uint32_t n, const Grid& g, float2* xy, uint32_t* out_tag,

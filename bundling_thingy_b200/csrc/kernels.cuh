@@ -113,8 +113,10 @@ void launch_cell_table(const uint32_t* hist, size_t cells, uint32_t* cell_start,
                        bool tiles_ready, cudaStream_t s);
 
 // Pairs of samples sharing a grid cell (r x r texels): sum over grid cells of
-// n (n - 1), from the search-cell populations; added to *out.
-void launch_grid_pairs(const uint32_t* hist, const Grid& g, unsigned long long* out, cudaStream_t s);
+// n (n - 1), from the search-cell populations; added to *out. scratch holds
+// gw * gh u32 (any contents).
+void launch_grid_pairs(const uint32_t* hist, const Grid& g, uint32_t* scratch, unsigned long long* out,
+                       cudaStream_t s);
 
 // Re-bins slot-order records under another search-cell shape: positions,
 // tags and new search cells in slot order (the scatter's input) and the new

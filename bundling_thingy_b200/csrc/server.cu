@@ -1,23 +1,25 @@
 // server.cu — continuous batching of arriving bundling requests (bt_server_*).
 //
-// One worker thread owns one bt_batch and every device context. Each turn of
-// its loop:
-//   1. requests whose arrival time has passed join the ready queue (arrival
-//      order);
-//   2. admission: while `max_active` and the device-memory budget allow, the
-//      head of the queue takes an idle context of the same options (or a new
-//      one) and starts its upload — the count phase of Gpu::upload, on the
-//      context's own stream;
-//   3. the batch advances every running graph by `step` iterations (one CUDA
-//      graph launch per iteration on the batch's stream), step = the smallest
-//      remaining iteration count, at most `max_step`;
-//   4. meanwhile the admitted uploads finish (emit, density pass 0, first
-//      binning), are checked and join the batch for the next turn;
-//   5. after the batch's step, every graph that reached its iteration count
-//      leaves the batch: its positions are unsorted into records on its own
-//      stream and the request is finished. Its memory stays charged until the
-//      client releases it; released contexts are kept idle for reuse by the
-//      next request with the same options (and freed when memory is short).
+// One worker thread owns one bt_batch and every device context, and never
+// blocks on the device while there is work to move: it polls events.
+//   - Requests whose arrival time has passed join the ready queue (arrival
+//     order).
+//   - A batch step starts as soon as the previous one has finished: every
+//     running graph advances by `step` iterations (one CUDA graph launch per
+//     iteration on the batch's stream), step = the smallest remaining
+//     iteration count, at most `max_step`.
+//   - Admission: while `max_active` and the device-memory budget allow, the
+//     head of the queue takes an idle context of the same options (or a new
+//     one) and starts its upload on the context's own stream. Each upload
+//     phase (count; emit, density pass 0 and first binning; check and
+//     search-cell shape) starts when the previous one is done, beside the
+//     running step; a loaded graph joins the batch for the next step.
+//   - After a step, every graph that reached its iteration count leaves the
+//     batch and its positions are unsorted into records on its own stream;
+//     the request is finished when they are ready. Its memory stays charged
+//     until the client releases it; released contexts are kept idle for reuse
+//     by the next request with the same options (and freed when memory is
+//     short).
 //
 // Admission generalises Allocation::new (src/resampling.rs:321-397) from one
 // graph to all resident graphs: each context charges its device allocations
@@ -76,6 +78,7 @@ struct bt_server {
     bt_server_options opt{};
     bt::MemAccount account;
     bt_batch* batch = nullptr;
+    cudaEvent_t step_done = nullptr;   // end of the batch step in flight
     std::chrono::steady_clock::time_point t0;
     std::thread worker;
 
@@ -94,7 +97,8 @@ struct bt_server {
     // Worker-only state.
     std::vector<Request*> future;    // arrival time not reached, sorted by (arrival, id)
     std::deque<Request*> ready;      // arrived, waiting for admission, sorted by (arrival, id)
-    std::vector<Request*> counting, running;
+    std::vector<Request*> uploading, running;   // uploading: Counting or Loading
+    std::vector<Request*> finishing;   // out of the batch, records being unsorted
     std::vector<bt_ctx*> pool;       // idle contexts
 
     double now() const { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); }
@@ -154,6 +158,12 @@ void fail_request(bt_server* s, Request* r, bt_status status, const std::string&
 }
 
 bool evict_idle(bt_server* s) {
+    {
+        // Contexts the client released since the turn began are idle too.
+        std::lock_guard<std::mutex> lk(s->mu);
+        for (bt_ctx* c : s->released) s->pool.push_back(c);
+        s->released.clear();
+    }
     if (s->pool.empty()) return false;
     bt_destroy(s->pool.front());
     s->pool.erase(s->pool.begin());
@@ -181,8 +191,9 @@ bt_ctx* take_idle(bt_server* s, const bt_options& o) {
 bool others_hold_memory(bt_server* s, const Request* self) {
     for (const Request* r : s->running)
         if (r != self) return true;
-    for (const Request* r : s->counting)
+    for (const Request* r : s->uploading)
         if (r != self) return true;
+    if (!s->finishing.empty()) return true;
     std::lock_guard<std::mutex> lk(s->mu);
     return s->stats.resident_results > 0;
 }
@@ -200,24 +211,55 @@ Budget on_budget(bt_server* s, const Request* r) {
     return Budget::Fail;
 }
 
-size_t active_count(const bt_server* s) { return s->counting.size() + s->running.size(); }
+size_t active_count(const bt_server* s) { return s->uploading.size() + s->running.size(); }
 
-// Step 2: start the uploads of the head of the ready queue.
-void admit(bt_server* s) {
+// Records the end of the work queued so far on a context's stream.
+bool mark(bt_ctx* c) { return cudaEventRecord(c->done, c->stream) == cudaSuccess; }
+
+// 1 when the marked work is done, 0 while it runs, -1 on a device error.
+int marked_done(bt_ctx* c) {
+    const cudaError_t e = cudaEventQuery(c->done);
+    if (e == cudaSuccess) return 1;
+    if (e == cudaErrorNotReady) return 0;
+    return -1;
+}
+
+// Back to the ready queue in arrival order; its context stays idle and
+// evictable, so a graph that fits alone always progresses.
+void requeue(bt_server* s, Request* r) {
+    s->pool.push_back(r->ctx);
+    r->ctx = nullptr;
+    r->state = State::Pending;
+    s->ready.insert(std::upper_bound(s->ready.begin(), s->ready.end(), r, by_arrival), r);
+    std::lock_guard<std::mutex> lk(s->mu);
+    ++s->stats.budget_waits;
+}
+
+// Starts the uploads of the head of the ready queue; returns whether any
+// started (or failed).
+bool admit(bt_server* s) {
+    bool moved = false;
     while (!s->ready.empty()) {
-        if (s->opt.max_active && active_count(s) >= s->opt.max_active) return;
+        if (s->opt.max_active && active_count(s) >= s->opt.max_active) return moved;
         Request* r = s->ready.front();
         bt_ctx* c = take_idle(s, r->opt);
         if (!c) {
+            const double t0 = s->now();
             bt_status st = bt::create_context(&r->opt, &s->account, &c);
+            {
+                std::lock_guard<std::mutex> lk(s->mu);
+                s->stats.create_s += s->now() - t0;
+                if (st == BT_OK) ++s->stats.contexts_created;
+            }
             if (st == BT_ERR_BUDGET) {
                 const Budget b = on_budget(s, r);
                 if (b == Budget::Retry) continue;
-                if (b == Budget::Defer) return;
+                if (b == Budget::Defer) return moved;
             }
             if (st != BT_OK) {
                 s->ready.pop_front();
                 fail_request(s, r, st, bt_last_error(nullptr));
+                moved = true;
                 continue;
             }
         }
@@ -229,121 +271,145 @@ void admit(bt_server* s) {
             r->ctx = nullptr;
             const Budget b = on_budget(s, r);
             if (b == Budget::Retry) continue;
-            if (b == Budget::Defer) return;
+            if (b == Budget::Defer) return moved;
         }
         s->ready.pop_front();
-        if (st != BT_OK) {
+        moved = true;
+        if (st != BT_OK || !mark(c)) {
             const std::string msg = c->err;
-            fail_request(s, r, st, msg);
+            fail_request(s, r, st ? st : BT_ERR_CUDA, msg);
             continue;
         }
         r->state = State::Counting;
         r->result.admitted_s = s->now();
-        s->counting.push_back(r);
+        s->uploading.push_back(r);
     }
+    return moved;
 }
 
-// Step 4: finish the admitted uploads and join them to the batch. Requests
-// refused by the budget go back to the ready queue.
-void finish_uploads(bt_server* s) {
-    if (s->counting.empty()) return;
-    std::vector<Request*> batch_of(s->counting);
-    s->counting.clear();
-    std::vector<Request*> loading;
-    for (Request* r : batch_of) {
-        if (bt_status st = bt::upload_wait(r->ctx)) {
-            const std::string msg = r->ctx->err;
-            fail_request(s, r, st, msg);
+// Uploads move on without blocking: each phase is launched when the previous
+// one's work is done on the request's stream. Requests refused by the budget
+// go back to the ready queue. Returns whether anything moved.
+bool advance_uploads(bt_server* s) {
+    bool moved = false;
+    std::vector<Request*> still;
+    for (size_t k = 0; k < s->uploading.size(); ++k) {
+        Request* r = s->uploading[k];
+        const int done = marked_done(r->ctx);
+        if (done == 0) {
+            still.push_back(r);
             continue;
         }
-        loading.push_back(r);
-    }
-    // Another graph of this turn that is still uploading or loaded holds
-    // memory it will give back when it finishes.
-    auto wave_holds = [&](const Request* self) {
-        for (const Request* q : batch_of)
-            if (q != self && q->ctx && (q->state == State::Counting || q->state == State::Loading)) return true;
-        return false;
-    };
-    std::vector<Request*> loaded;
-    for (Request* r : loading) {
-        bt_status st = bt::upload_finish(r->ctx);
-        while (st == BT_ERR_BUDGET && evict_idle(s)) st = bt::upload_finish(r->ctx);
-        if (st == BT_ERR_BUDGET && (wave_holds(r) || others_hold_memory(s, r))) {
-            // Graphs of this turn, running graphs or held results will give
-            // memory back: requeue in arrival order (the context stays idle
-            // and evictable, so a graph that fits alone always progresses).
-            s->pool.push_back(r->ctx);
-            r->ctx = nullptr;
-            r->state = State::Pending;
-            s->ready.insert(std::upper_bound(s->ready.begin(), s->ready.end(), r, by_arrival), r);
-            std::lock_guard<std::mutex> lk(s->mu);
-            ++s->stats.budget_waits;
+        moved = true;
+        if (done < 0) {
+            fail_request(s, r, BT_ERR_CUDA, std::string("device execution: ") + cudaGetErrorString(cudaGetLastError()));
             continue;
         }
-        if (st != BT_OK) {
-            const std::string msg = r->ctx->err;
-            fail_request(s, r, st, msg);
+        auto others = [&] {
+            for (size_t q = k + 1; q < s->uploading.size(); ++q)
+                if (s->uploading[q]->ctx) return true;
+            return !still.empty() || others_hold_memory(s, r);
+        };
+        if (r->state == State::Counting) {
+            bt_status st = bt::upload_finish(r->ctx);
+            while (st == BT_ERR_BUDGET && evict_idle(s)) st = bt::upload_finish(r->ctx);
+            if (st == BT_ERR_BUDGET && others()) {
+                requeue(s, r);
+                continue;
+            }
+            if (st != BT_OK || !mark(r->ctx)) {
+                const std::string msg = r->ctx->err;
+                fail_request(s, r, st ? st : BT_ERR_CUDA, msg);
+                continue;
+            }
+            r->state = State::Loading;
+            still.push_back(r);
             continue;
         }
-        r->state = State::Loading;
-        loaded.push_back(r);
-    }
-    for (Request* r : loaded) {
+        // Loaded: check, pick the search-cell shape, keep room for the records.
         uint32_t samples = 0;
-        bt_status st = bt::upload_wait(r->ctx);
-        if (st == BT_OK) st = bt::upload_check(r->ctx, &samples);
+        bt_status st = bt::upload_check(r->ctx, &samples);
         if (st == BT_OK) st = bt::upload_adapt(r->ctx);
-        if (st == BT_OK) st = bt::reserve_records(r->ctx);
-        if (st == BT_OK && r->iterations == 0) {
-            // Nothing to iterate: the upload is the result.
-            st = bt::prepare_records(r->ctx);
-            if (st == BT_OK) st = bt::upload_wait(r->ctx);
-            if (st == BT_OK) {
-                publish(s, r, BT_OK, "");
+        if (st == BT_OK) {
+            st = bt::reserve_records(r->ctx);
+            while (st == BT_ERR_BUDGET && evict_idle(s)) st = bt::reserve_records(r->ctx);
+            if (st == BT_ERR_BUDGET && others()) {
+                requeue(s, r);
                 continue;
             }
         }
-        if (st == BT_OK) st = bt::batch_attach(s->batch, r->ctx, &r->slot);
+        if (st == BT_OK && r->iterations == 0) {
+            // Nothing to iterate: the upload is the result.
+            st = bt::prepare_records(r->ctx);
+            if (st == BT_OK && mark(r->ctx)) {
+                s->finishing.push_back(r);
+                continue;
+            }
+        }
         if (st != BT_OK) {
-            const std::string msg = bt_batch_last_error(s->batch)[0] ? bt_batch_last_error(s->batch) : r->ctx->err;
+            const std::string msg = r->ctx->err;
             fail_request(s, r, st, msg);
+            continue;
+        }
+        if (bt_status ast = bt::batch_attach(s->batch, r->ctx, &r->slot)) {
+            fail_request(s, r, ast, bt_batch_last_error(s->batch));
             continue;
         }
         r->state = State::Running;
         s->running.push_back(r);
     }
+    s->uploading.swap(still);
+    return moved;
 }
 
-// Step 5: graphs that reached their iteration count leave the batch.
-void complete(bt_server* s) {
-    std::vector<Request*> still, done;
-    for (Request* r : s->running) (r->ctx->iterations >= r->iterations ? done : still).push_back(r);
-    if (done.empty()) return;
-    s->running.swap(still);
-    for (Request* r : done) {
-        bt_ctx* c = bt::batch_detach(s->batch, r->slot);
-        bt_status st = c ? bt::prepare_records(c) : BT_ERR_CUDA;
-        if (!c) {
-            r->ctx = nullptr;
-            publish(s, r, st, "batch slot lost");
+// Graphs that reached their iteration count leave the batch after its step;
+// their records are unsorted on their own streams.
+void retire(bt_server* s) {
+    std::vector<Request*> still;
+    for (Request* r : s->running) {
+        if (r->ctx->iterations < r->iterations) {
+            still.push_back(r);
             continue;
         }
-        if (st != BT_OK) {
+        bt_ctx* c = bt::batch_detach(s->batch, r->slot);
+        if (!c) {
+            r->ctx = nullptr;
+            publish(s, r, BT_ERR_CUDA, "batch slot lost");
+            continue;
+        }
+        if (bt_status st = bt::prepare_records(c)) {
             const std::string msg = c->err;
             fail_request(s, r, st, msg);
+            continue;
         }
+        if (!mark(c)) {
+            fail_request(s, r, BT_ERR_CUDA, "cudaEventRecord");
+            continue;
+        }
+        s->finishing.push_back(r);
     }
-    for (Request* r : done) {
-        if (!r->ctx || r->state != State::Running) continue;
-        bt_status st = bt::upload_wait(r->ctx);
-        if (st != BT_OK) {
-            const std::string msg = r->ctx->err;
-            fail_request(s, r, st, msg);
+    s->running.swap(still);
+}
+
+// Requests whose records are ready are finished. Returns whether any was.
+bool publish_ready(bt_server* s) {
+    bool moved = false;
+    std::vector<Request*> still;
+    for (Request* r : s->finishing) {
+        const int done = marked_done(r->ctx);
+        if (done == 0) {
+            still.push_back(r);
+            continue;
+        }
+        moved = true;
+        if (done < 0) {
+            fail_request(s, r, BT_ERR_CUDA, std::string("device execution: ") + cudaGetErrorString(cudaGetLastError()));
             continue;
         }
         publish(s, r, BT_OK, "");
     }
+    s->finishing.swap(still);
+    return moved;
 }
 
 void fail_running(bt_server* s, bt_status st, const std::string& msg) {
@@ -358,8 +424,10 @@ void fail_running(bt_server* s, bt_status st, const std::string& msg) {
 
 void worker_main(bt_server* s) {
     cudaSetDevice(s->opt.device);
+    double t_launch = 0, t_upload = 0, t_wait = 0, t_retire = 0, t_idle = 0;
+    bool step_busy = false;
     for (;;) {
-        // 1. Arrivals and releases.
+        // Arrivals and releases.
         {
             std::unique_lock<std::mutex> lk(s->mu);
             if (s->stop) break;
@@ -377,58 +445,81 @@ void worker_main(bt_server* s) {
                             s->future[i]);
         s->future.erase(s->future.begin(), s->future.begin() + static_cast<std::ptrdiff_t>(arrived));
 
-        // 2. Admission.
-        admit(s);
-
-        // 3. One batch step over the running graphs.
-        uint32_t step = 0;
-        if (!s->running.empty()) {
-            step = std::max<uint32_t>(1, s->opt.max_step);
+        double mark_t = s->now();
+        auto lap = [&](double& acc) {
+            const double now = s->now();
+            acc += now - mark_t;
+            mark_t = now;
+        };
+        bool moved = false;
+        // The next batch step as soon as the previous one is done.
+        if (!step_busy && !s->running.empty()) {
+            uint32_t step = std::max<uint32_t>(1, s->opt.max_step);
             for (const Request* r : s->running) step = std::min(step, r->iterations - r->ctx->iterations);
             if (bt_status st = bt_batch_iterate_async(s->batch, step)) {
                 fail_running(s, st, bt_batch_last_error(s->batch));
-                step = 0;
+            } else if (cudaEventRecord(s->step_done, bt::batch_stream(s->batch)) != cudaSuccess) {
+                fail_running(s, BT_ERR_CUDA, "cudaEventRecord");
+            } else {
+                step_busy = true;
+                std::lock_guard<std::mutex> lk(s->mu);
+                ++s->stats.steps;
             }
+            moved = true;
+            lap(t_launch);
         }
-
-        // 4. Uploads finish while the batch iterates.
-        finish_uploads(s);
-
-        // 5. Completions.
-        if (step) {
+        moved |= publish_ready(s);
+        lap(t_retire);
+        moved |= admit(s);
+        moved |= advance_uploads(s);
+        lap(t_upload);
+        if (step_busy && cudaEventQuery(s->step_done) != cudaErrorNotReady) {
+            step_busy = false;
+            moved = true;
             if (bt_status st = bt_batch_synchronize(s->batch)) {
                 fail_running(s, st, bt_batch_last_error(s->batch));
             } else {
-                complete(s);
+                retire(s);
             }
+            lap(t_retire);
         }
         {
             std::lock_guard<std::mutex> lk(s->mu);
-            if (step) ++s->stats.steps;
             s->stats.queued = static_cast<uint32_t>(s->ready.size() + s->future.size() + s->incoming.size());
             s->stats.active = static_cast<uint32_t>(active_count(s));
             s->stats.peak_active = std::max(s->stats.peak_active, s->stats.active);
             s->stats.device_bytes = s->account.used.load();
             s->stats.peak_device_bytes = std::max(s->stats.peak_device_bytes, s->stats.device_bytes);
+            s->stats.launch_s = t_launch;
+            s->stats.upload_s = t_upload;
+            s->stats.wait_s = t_wait;
+            s->stats.retire_s = t_retire;
+            s->stats.idle_s = t_idle;
         }
-
+        if (moved) continue;
+        if (step_busy || !s->uploading.empty() || !s->finishing.empty()) {
+            // Device work in flight: poll again shortly.
+            std::this_thread::sleep_for(std::chrono::microseconds(20));
+            lap(t_wait);
+            continue;
+        }
         // Idle: sleep until the next arrival, a submission or a release.
-        if (s->running.empty() && s->counting.empty()) {
-            std::unique_lock<std::mutex> lk(s->mu);
-            if (s->stop) break;
-            if (!s->incoming.empty() || !s->released.empty()) continue;
-            if (!s->ready.empty()) {
-                // Waiting on the budget: a release wakes us.
-                s->work_cv.wait_for(lk, std::chrono::milliseconds(50));
-            } else if (!s->future.empty()) {
-                const double wait_s = s->future.front()->arrival - s->now();
-                if (wait_s > 0)
-                    s->work_cv.wait_for(lk, std::chrono::duration<double>(std::min(wait_s, 0.05)));
-            } else {
-                s->work_cv.wait_for(lk, std::chrono::milliseconds(50));
-            }
+        std::unique_lock<std::mutex> lk(s->mu);
+        if (s->stop) break;
+        if (!s->incoming.empty() || !s->released.empty()) continue;
+        if (!s->ready.empty()) {
+            // Waiting on the budget: a release wakes us.
+            s->work_cv.wait_for(lk, std::chrono::milliseconds(50));
+        } else if (!s->future.empty()) {
+            const double wait_s = s->future.front()->arrival - s->now();
+            if (wait_s > 0) s->work_cv.wait_for(lk, std::chrono::duration<double>(std::min(wait_s, 0.05)));
+        } else {
+            s->work_cv.wait_for(lk, std::chrono::milliseconds(50));
         }
+        lk.unlock();
+        lap(t_idle);
     }
+    if (step_busy) bt_batch_synchronize(s->batch);   // bounded wait
 }
 
 }  // namespace
@@ -457,6 +548,11 @@ bt_status bt_server_create(const bt_server_options* options, bt_server** out) {
         delete s;
         return sfail(nullptr, st, msg);
     }
+    if (cudaEventCreateWithFlags(&s->step_done, cudaEventDisableTiming) != cudaSuccess) {
+        bt_batch_destroy(s->batch);
+        delete s;
+        return sfail(nullptr, BT_ERR_CUDA, "cudaEventCreate");
+    }
     s->t0 = std::chrono::steady_clock::now();
     s->worker = std::thread(worker_main, s);
     *out = s;
@@ -482,6 +578,7 @@ void bt_server_destroy(bt_server* s) {
     for (bt_ctx* c : s->pool) bt_destroy(c);
     for (bt_ctx* c : s->released) bt_destroy(c);
     bt_batch_destroy(s->batch);
+    if (s->step_done) cudaEventDestroy(s->step_done);
     delete s;
 }
 

@@ -262,6 +262,12 @@ typedef struct bt_server_stats {
     uint64_t steps, rebuilds, budget_waits, evictions;
     uint32_t queued, active, peak_active, resident_results;
     uint64_t device_bytes, peak_device_bytes;
+    /* Seconds the worker spent launching batch steps (with rebuilds),
+     * uploading (admission and upload phases), waiting for steps, retiring
+     * and publishing finished graphs, and idle. */
+    double launch_s, upload_s, wait_s, retire_s, idle_s;
+    uint64_t contexts_created;   /* device contexts made (the rest were reused) */
+    double create_s;             /* of upload_s: seconds spent making contexts */
 } bt_server_stats;
 
 /* device 0, max_active 32, budget 120 GB (120e9 bytes), max_step 1. */

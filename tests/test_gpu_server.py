@@ -92,8 +92,9 @@ def test_budget_defers_admission_and_results_stay_exact():
     budget = int(one * 1.5)               # room for one such graph at a time
     server = bt.Server(max_active=8, budget_bytes=budget)
     expected = {}
+    t0 = server.clock() + 0.05              # all three become ready together
     for iters in (3, 2, 4):
-        expected[server.submit(o, mid.xy, mid.starts, iters)] = (mid, o, iters)
+        expected[server.submit(o, mid.xy, mid.starts, iters, arrival_s=t0)] = (mid, o, iters)
     drain(server, len(expected), expected)
     st = server.stats()
     assert st["peak_device_bytes"] <= budget
