@@ -425,9 +425,14 @@ class Gpu:
         self._ck(library().bt_read_edges(self._h, _p(out, _f32p), out.size))
         return out
 
-    def read_density(self) -> np.ndarray:
+    def read_density(self, out: np.ndarray | None = None) -> np.ndarray:
+        """The normalised density map (width * height f32); `out`, when given,
+        is a C-contiguous f32 host array of that size (pinned reads fastest)."""
         o = self.options
-        out = np.zeros(o.width * o.height, np.float32)
+        if out is None:
+            out = np.zeros(o.width * o.height, np.float32)
+        elif out.dtype != np.float32 or out.size != o.width * o.height or not out.flags.c_contiguous:
+            raise ValueError("density buffer must be C-contiguous f32 of width * height")
         self._ck(library().bt_read_density(self._h, _p(out, _f32p), out.size))
         return out
 

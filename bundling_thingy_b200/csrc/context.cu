@@ -153,7 +153,7 @@ void adaptive_shape(const bt_ctx* c, unsigned long long pairs, uint32_t* ky_out,
     const bt::Grid& g = c->grid;
     const double r = g.rf, n = static_cast<double>(c->samples);
     const double rho = std::max(static_cast<double>(pairs) / (r * r * n), 1e-4);
-    const double sy = std::min(std::max(3.75 / std::sqrt(rho), 0.25), std::min(4.0, r));
+    const double sy = std::min(std::max(4.5 / std::sqrt(rho), 0.25), std::min(4.0, r));
     uint32_t ky = static_cast<uint32_t>(std::min(std::max(std::lround(r / sy), 1L), 4096L));
     uint32_t kx = std::min(8u * ky, 4096u);
     // At most 32 Mi search cells (8 bytes each per iteration) and 8 per sample.

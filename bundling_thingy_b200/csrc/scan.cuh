@@ -57,11 +57,11 @@ __device__ __forceinline__ LL2 shfl_down<LL2>(LL2 v, int o) {
     return LL2{__shfl_down_sync(0xFFFFFFFFu, v.x, o), __shfl_down_sync(0xFFFFFFFFu, v.y, o)};
 }
 
-// Items per thread: tiles of 4096 elements of 4 bytes, 2048 up to 16 bytes,
-// 1024 above.
+// Items per thread: tiles of 2048 elements up to 8 bytes, 1024 above (16-byte
+// sums: fewer registers per thread, more resident blocks).
 template <typename T>
 __host__ __device__ constexpr int scan_items() {
-    return sizeof(T) <= 4 ? 16 : sizeof(T) <= 16 ? 8 : 4;
+    return sizeof(T) <= 8 ? 8 : 4;
 }
 template <typename T>
 __host__ __device__ constexpr size_t scan_tile() {
