@@ -50,6 +50,17 @@ struct MemAccount {
     uint64_t limit = 0;
 };
 
+// 64-byte host words in page-locked memory for the contexts' small status
+// and count read-backs, carved from shared slabs (one cudaMallocHost per 256
+// contexts instead of two per context). Thread-safe.
+void* pinned_slot();
+void release_pinned_slot(void* p);
+
+// Once per device: the stream-ordered allocator keeps freed memory for
+// reuse instead of returning it to the driver at each synchronisation, and
+// reuses it across streams only where the streams are already ordered.
+cudaError_t prepare_device_memory(int device);
+
 // bt_create with an optional shared account (nullptr = unaccounted).
 bt_status create_context(const bt_options* options, MemAccount* account, bt_ctx** out);
 
