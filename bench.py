@@ -64,6 +64,7 @@ def parse_args():
     p.add_argument("--max-active", type=int, default=32)
     p.add_argument("--max-step", type=int, default=1)
     p.add_argument("--budget-gb", type=float, default=120.0)
+    p.add_argument("--reserve-gb", type=float, default=48.0, help="served workload: device memory mapped at start")
     return p.parse_args()
 
 
@@ -579,7 +580,7 @@ def run_served(args, ranks: Ranks):
 
     def served_run(sched):
         server = bt.Server(device, max_active=args.max_active, budget_bytes=int(args.budget_gb * 1e9),
-                           max_step=args.max_step)
+                           max_step=args.max_step, reserve_bytes=int(args.reserve_gb * 1e9))
         # Warm-up to the steady state: the max_active largest requests at
         # once (kernels, device memory pool, idle contexts sized for large
         # graphs, like the plain loop's reused contexts).
@@ -662,7 +663,7 @@ def run_served(args, ranks: Ranks):
         "config": {"workload": f"served: {n} Poisson requests per rank at {args.rate:g}/s, edges log-uniform "
                                f"500-50k, grids 512/1024/2048, {iters} iterations, "
                                f"{args.budget_gb:g} GB admission budget",
-                   "max_active": args.max_active, "max_step": args.max_step,
+                   "max_active": args.max_active, "max_step": args.max_step, "reserve_gb": args.reserve_gb,
                    "warm": "both arms warmed with the largest graphs first (device memory pool mapped, "
                            "contexts sized); inputs larger than L2",
                    "search_cells": "chosen per graph at upload from its density",

@@ -79,7 +79,8 @@ class _Info(ctypes.Structure):
 class _ServerOptions(ctypes.Structure):
     _fields_ = [
         ("device", ctypes.c_int32), ("max_active", ctypes.c_uint32), ("budget_bytes", ctypes.c_uint64),
-        ("max_step", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 7),
+        ("max_step", ctypes.c_uint32), ("reserved0", ctypes.c_uint32), ("reserve_bytes", ctypes.c_uint64),
+        ("reserved", ctypes.c_uint32 * 4),
     ]
 
 
@@ -630,10 +631,11 @@ class Server:
     iteration count is reached. Results stay on the device until released."""
 
     def __init__(self, device: int = 0, max_active: int = 32, budget_bytes: int = 120_000_000_000,
-                 max_step: int = 1):
+                 max_step: int = 1, reserve_bytes: int = 0):
         o = _ServerOptions()
         library().bt_server_options_init(ctypes.byref(o))
         o.device, o.max_active, o.budget_bytes, o.max_step = device, max_active, budget_bytes, max_step
+        o.reserve_bytes = reserve_bytes
         h = _vp()
         _check(library().bt_server_create(ctypes.byref(o), ctypes.byref(h)))
         self._h = h

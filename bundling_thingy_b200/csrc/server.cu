@@ -7,7 +7,7 @@
 //   - A batch step starts as soon as the previous one has finished: every
 //     running graph advances by `step` iterations (one CUDA graph launch per
 //     iteration on the batch's stream), step = the smallest remaining
-//     iteration count, at most `max_step`.
+//     iteration count, at most `max_step` while other requests wait to join.
 //   - Admission: while `max_active` and the device-memory budget allow, the
 //     head of the queue takes an idle context of the same options (or a new
 //     one) and starts its upload on the context's own stream. Each upload
@@ -454,7 +454,10 @@ void worker_main(bt_server* s) {
         bool moved = false;
         // The next batch step as soon as the previous one is done.
         if (!step_busy && !s->running.empty()) {
-            uint32_t step = std::max<uint32_t>(1, s->opt.max_step);
+            // Nothing waiting to join: run the running graphs up to the first
+            // one's end in one launch sequence (no host turn per iteration).
+            const bool joining = !s->ready.empty() || !s->uploading.empty();
+            uint32_t step = joining ? std::max<uint32_t>(1, s->opt.max_step) : UINT32_MAX;
             for (const Request* r : s->running) step = std::min(step, r->iterations - r->ctx->iterations);
             if (bt_status st = bt_batch_iterate_async(s->batch, step)) {
                 fail_running(s, st, bt_batch_last_error(s->batch));
@@ -552,6 +555,25 @@ bt_status bt_server_create(const bt_server_options* options, bt_server** out) {
         bt_batch_destroy(s->batch);
         delete s;
         return sfail(nullptr, BT_ERR_CUDA, "cudaEventCreate");
+    }
+    if (options->reserve_bytes) {
+        // Map the reserve into the stream-ordered pool once: an allocation
+        // that grows the pool while batch steps run stalls the worker.
+        const uint64_t bytes = std::min(options->reserve_bytes, options->budget_bytes);
+        cudaError_t e = bt::prepare_device_memory(options->device);
+        const cudaStream_t st = bt::batch_stream(s->batch);
+        void* p = nullptr;
+        if (e == cudaSuccess) e = cudaMallocAsync(&p, bytes, st);
+        if (e == cudaSuccess) e = cudaFreeAsync(p, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            cudaEventDestroy(s->step_done);
+            bt_batch_destroy(s->batch);
+            delete s;
+            return sfail(nullptr, e == cudaErrorMemoryAllocation ? BT_ERR_BUDGET : BT_ERR_CUDA,
+                         std::string("device memory reserve: ") + cudaGetErrorString(e));
+        }
     }
     s->t0 = std::chrono::steady_clock::now();
     s->worker = std::thread(worker_main, s);

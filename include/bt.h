@@ -240,8 +240,12 @@ typedef struct bt_server_options {
     int32_t device;
     uint32_t max_active;      /* graphs uploading or iterating at once (0 = unlimited) */
     uint64_t budget_bytes;    /* device memory of all resident graphs and pooled contexts */
-    uint32_t max_step;        /* batch iterations between admission points (>= 1) */
-    uint32_t reserved[7];
+    uint32_t max_step;        /* batch iterations between admission points while requests wait to join (>= 1) */
+    uint32_t reserved0;
+    uint64_t reserve_bytes;   /* device memory mapped into the allocator's pool at creation, so that
+                                 admissions do not map memory while steps run (0 = none; at most
+                                 budget_bytes) */
+    uint32_t reserved[4];
 } bt_server_options;
 
 typedef struct bt_request_result {
@@ -270,7 +274,7 @@ typedef struct bt_server_stats {
     double create_s;             /* of upload_s: seconds spent making contexts */
 } bt_server_stats;
 
-/* device 0, max_active 32, budget 120 GB (120e9 bytes), max_step 1. */
+/* device 0, max_active 32, budget 120 GB (120e9 bytes), max_step 1, no reserve. */
 void bt_server_options_init(bt_server_options* options);
 bt_status bt_server_create(const bt_server_options* options, bt_server** out);
 /* Stops the worker; unfinished requests are dropped. */

@@ -34,6 +34,8 @@ def test_abi_version(lib):
     # The ctypes mirrors keep the C layouts (no padding holes in either).
     assert ctypes.sizeof(bt._Options) == 88
     assert ctypes.sizeof(bt._Info) == 64
+    assert ctypes.sizeof(bt._ServerOptions) == 48
+    assert bt._ServerOptions.reserve_bytes.offset == 24
 
 
 def test_options_defaults_match_reference(lib):
