@@ -7,6 +7,8 @@ the same f32 operation sequence; the stated tolerances (1e-4 of the canvas
 extent = 2e-4 clip units for positions, 1e-5 relative for density) are the
 contract and are asserted as well.
 """
+import json
+
 import numpy as np
 import pytest
 
@@ -379,3 +381,43 @@ def test_upload_picks_flat_search_cells_for_dense_graphs(oracle):
     ora.iterate(2)
     check_points(gpu, ora)
     check_density(gpu, ora)
+
+
+def test_headless_distortion_report(oracle, tmp_path, capsys):
+    # The headless run's distortion.json (src/main.rs:104-191): the device and
+    # host measurements agree, and iteration 3 matches the oracle.
+    from bundling_thingy_b200 import report
+
+    w = synthetic.small()
+    trl = tmp_path / "g.trl"
+    synthetic.write_trl(trl, w.xy, w.starts)
+    base = dict(width=w.width, height=w.height, sample_spacing=w.spacing, blur_sigma=w.sigma,
+                blur_shrink=w.shrink)
+    (tmp_path / "out").mkdir()
+    (tmp_path / "out" / "distortion.json").write_text("stale")
+    r_dev = report.headless_distortion(trl, tmp_path / "out", neighbor_radius=w.radius, iterations=3,
+                                       options=bt.Options(**base))
+    printed = capsys.readouterr().out.splitlines()
+    assert printed[0] == "original.png distortion=0 rms_displacement_pixels=0"
+    assert printed[1].startswith("iteration-01.png distortion=")
+    r_host = report.headless_distortion(trl, tmp_path / "host", neighbor_radius=w.radius, iterations=3,
+                                        options=bt.Options(**base), measure="host", echo=False)
+    assert [i["file"] for i in r_dev["images"]] == ["original.png", "iteration-01.png", "iteration-02.png",
+                                                    "iteration-03.png"]
+    for a, b in zip(r_dev["images"], r_host["images"]):
+        assert abs(a["distortion"] - b["distortion"]) <= 1e-12 * max(b["distortion"], 1e-30)
+        assert abs(a["rms_displacement_pixels"] - b["rms_displacement_pixels"]) <= \
+            1e-12 * max(b["rms_displacement_pixels"], 1e-30)
+    assert json.loads((tmp_path / "out" / "distortion.json").read_text()) == r_dev
+    assert r_dev["bundling"] == {"neighbor_radius": w.radius, "iterations": 3}
+    # Iteration 3 against the oracle run of the same parsed graph.
+    g = bt.Graph.load(trl)
+    o = bt.Options(neighbor_radius=w.radius, evaluate_distortion=True, **base)
+    gpu, ora = pair(oracle, g.points(), g.starts(), o)
+    b0, _ = ora.points()
+    ora.iterate(3)
+    d, px = oracle.distortion(ora.paths(), b0, ora.points()[0], bt.SIZE)
+    last = r_dev["images"][-1]
+    assert abs(last["distortion"] - d) <= 1e-12 * d
+    assert abs(last["rms_displacement_pixels"] - px) <= 1e-12 * px
+    assert r_dev["geometry"]["active_samples"] == gpu.info().samples
