@@ -26,6 +26,7 @@ import numpy as np
 __all__ = [
     "BtError", "Options", "Graph", "Gpu", "Batch", "Info", "Layout", "Snapshot", "Aggregate", "Measurement",
     "squared_integral", "library", "library_path", "build", "COLOR_BY_DENSITY", "COLOR_BY_EDGE_ID", "SIZE",
+    "Frame", "PALETTES",
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -33,11 +34,13 @@ _LIB = os.path.join(_HERE, "libbt.so")
 SIZE = 1600                      # headless canvas of the reference (src/gpu.rs:21)
 COLOR_BY_DENSITY = 0
 COLOR_BY_EDGE_ID = 1
+PALETTES = ("viridis", "cividis", "plasma", "batlow")   # bt_options.palette index -> --palette name
 
 _f32p = ctypes.POINTER(ctypes.c_float)
 _u32p = ctypes.POINTER(ctypes.c_uint32)
 _f64p = ctypes.POINTER(ctypes.c_double)
 _vp = ctypes.c_void_p
+_u8p = ctypes.POINTER(ctypes.c_uint8)
 
 STATUS = {
     0: "ok", 1: "capacity overflow", 2: "count/emit mismatch", 3: "invalid input", 4: "no graph",
@@ -62,7 +65,8 @@ class _Options(ctypes.Structure):
         ("sample_spacing", ctypes.c_float), ("blur_sigma", ctypes.c_float), ("blur_shrink", ctypes.c_float),
         ("fine_cells", ctypes.c_uint32), ("use_graphs", ctypes.c_uint32), ("timing", ctypes.c_uint32),
         ("record_neighbors", ctypes.c_uint32), ("search_mode", ctypes.c_uint32), ("fine_cells_x", ctypes.c_uint32),
-        ("reserved", ctypes.c_uint32 * 5),
+        ("palette", ctypes.c_uint32), ("msaa", ctypes.c_uint32), ("endpoint_dots", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32 * 2),
     ]
 
 
@@ -130,6 +134,7 @@ SIGNATURES = {
     "bt_read_binning": ([_vp, _u32p, ctypes.c_size_t, _u32p, ctypes.c_size_t], ctypes.c_int32),
     "bt_read_neighbors": ([_vp, _u32p, ctypes.c_size_t], ctypes.c_int32),
     "bt_distortion": ([_vp, ctypes.c_uint32, _f64p, _f64p], ctypes.c_int32),
+    "bt_render": ([_vp, _u8p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_uint64), _f32p], ctypes.c_int32),
     "bt_stage_times": ([_vp, ctypes.POINTER(ctypes.c_char_p), _f32p, ctypes.c_uint32, _u32p], ctypes.c_int32),
     "bt_density_noalloc": ([_vp, _vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_float, _vp], ctypes.c_int32),
     "bt_autotune": ([ctypes.POINTER(_Options), _f32p, ctypes.c_uint32, _u32p, ctypes.c_uint32, ctypes.c_uint32,
@@ -235,6 +240,9 @@ class Options:
     record_neighbors: bool = False
     search_mode: int = 0     # 0: interior cells by prefix sums; 1: test every candidate (same results)
     fine_cells_x: int = 0    # search cells per grid cell along x (0 = fine_cells)
+    palette: int = 0         # PALETTES index (src/palette.rs:13-23): viridis, the reference default
+    msaa: int = 4            # samples per pixel: 2 or 4 as the reference (1 accepted)
+    endpoint_dots: bool = False
 
     def _struct(self) -> _Options:
         o = _Options()
@@ -254,6 +262,9 @@ class Options:
         o.record_neighbors = int(bool(self.record_neighbors))
         o.search_mode = int(self.search_mode)
         o.fine_cells_x = self.fine_cells_x
+        o.palette = int(self.palette)
+        o.msaa = int(self.msaa)
+        o.endpoint_dots = int(bool(self.endpoint_dots))
         return o
 
     def resample_scale(self) -> tuple[float, float]:
@@ -473,6 +484,23 @@ class Gpu:
         r = ctypes.c_double()
         self._ck(library().bt_distortion(self._h, size, ctypes.byref(d), ctypes.byref(r)))
         return Measurement(d.value, r.value)
+
+    def render(self, out: np.ndarray | None = None, pixels: bool = True) -> "Frame":
+        """Gpu::render + Gpu::readback (src/gpu.rs:616-655): the frame as RGBA8
+        (height x width x 4, rows from the top), its count of pixels whose RGB
+        differs from the clear colour, and the device time of its kernels.
+        Before an upload this is the blank frame. pixels=False skips the copy."""
+        o = self.options
+        rgba = None
+        if pixels:
+            rgba = out if out is not None else np.empty((o.height, o.width, 4), np.uint8)
+            if rgba.dtype != np.uint8 or rgba.size != o.width * o.height * 4 or not rgba.flags.c_contiguous:
+                raise ValueError("out must be a contiguous uint8 array of height x width x 4")
+        colored = ctypes.c_uint64()
+        ms = np.zeros(1, np.float32)
+        self._ck(library().bt_render(self._h, _p(rgba, _u8p) if rgba is not None else None,
+                                     rgba.nbytes if rgba is not None else 0, ctypes.byref(colored), _p(ms, _f32p)))
+        return Frame(rgba, int(colored.value), float(ms[0]))
 
     def stage_times(self) -> dict[str, float]:
         cap = 64
@@ -709,6 +737,14 @@ class Server:
         st = _ServerStats()
         self._ck(library().bt_server_stats_get(self._h, ctypes.byref(st)))
         return {name: getattr(st, name) for name, _ in _ServerStats._fields_}
+
+
+@dataclass
+class Frame:
+    """A rendered frame (bt_render)."""
+    rgba: np.ndarray | None      # height x width x 4 uint8, rows from the top
+    colored_pixels: int          # pixels whose RGB differs from the clear colour
+    device_ms: float
 
 
 @dataclass

@@ -319,6 +319,9 @@ bt_status validate_options(const bt_options* o, bt_ctx* c) {
     if (o->neighbor_radius > 0 && (o->fine_cells > 4096 || o->fine_cells_x > 4096))
         return fail(c, BT_ERR_INVALID, "fine_cells too large");
     if (o->search_mode > 1) return fail(c, BT_ERR_INVALID, "unknown search_mode");
+    if (o->palette > BT_PALETTE_BATLOW) return fail(c, BT_ERR_INVALID, "unknown palette");
+    if (o->msaa != 0 && o->msaa != 1 && o->msaa != 2 && o->msaa != 4)
+        return fail(c, BT_ERR_INVALID, "msaa must be 1, 2 or 4 samples");
     const uint64_t grid = o->neighbor_radius ? reference_grid_bytes(o->width, o->height, o->neighbor_radius) : 0;
     const uint64_t staging = o->evaluate_distortion ? kDistortionStagingBytes : 0;
     // resampling.rs:85-89
@@ -416,7 +419,9 @@ void bt_destroy(bt_ctx* c) {
                       &c->neighbors, &c->baseline, &c->current, &c->sorted_rec[0], &c->sorted_rec[1],
                       &c->slot_prefix, &c->prefix_tiles, &c->sorted_tag[0], &c->sorted_tag[1], &c->hist,
                       &c->cell_start, &c->hist_tiles, &c->counts, &c->himg, &c->vimg, &c->norm, &c->peak,
-                      &c->records, &c->integrals};
+                      &c->records, &c->integrals, &c->r_seg_count, &c->r_seg_off, &c->r_scan64,
+                      &c->r_pair_tile, &c->r_pair_seg, &c->r_sorted, &c->r_hist, &c->r_hist_off, &c->r_scan32,
+                      &c->r_samples, &c->r_rgba, &c->r_misc};
     for (DevBuf* b : bufs) release(*b, c->stream);
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->account) c->account->used -= c->device_bytes;
@@ -1079,6 +1084,115 @@ bt_status bt_distortion(bt_ctx* c, uint32_t size, double* distortion, double* rm
     *rms_px = rms * (static_cast<double>(size) / 2.0);
     if (!std::isfinite(*distortion) || !std::isfinite(*rms_px))
         return fail(c, BT_ERR_INVALID, "nonfinite distortion measurement");
+    return BT_OK;
+}
+
+namespace {
+
+// One frame of bt_render with bin buffers for c->render_cap pairs; *pairs
+// receives the pairs the frame needed (above the capacity: nothing valid was
+// drawn and the caller grows the buffers and renders again).
+bt_status render_frame(bt_ctx* c, const float2* xy, bool timed, uint8_t* rgba, uint64_t* colored, uint64_t* pairs) {
+    const uint32_t w = c->opt.width, h = c->opt.height;
+    const size_t pixels = static_cast<size_t>(w) * h;
+    bt::RenderArgs a{};
+    a.w = w;
+    a.h = h;
+    a.ns = c->opt.msaa ? static_cast<int>(c->opt.msaa) : 4;
+    a.palette = static_cast<int>(c->opt.palette);
+    a.color_by_edge = c->opt.color_by == BT_COLOR_BY_EDGE_ID;
+    a.tile_shift = bt::render_tile_shift(w, h);
+    a.tiles_x = (w + (1u << a.tile_shift) - 1) >> a.tile_shift;
+    a.tiles_y = (h + (1u << a.tile_shift) - 1) >> a.tile_shift;
+    const size_t tiles = static_cast<size_t>(a.tiles_x) * a.tiles_y;
+    if (bt_status s = ensure(c, c->r_samples, 4 * pixels * a.ns)) return s;
+    if (bt_status s = ensure(c, c->r_rgba, 4 * pixels)) return s;
+    if (bt_status s = ensure(c, c->r_misc, 16)) return s;
+    a.samples = c->r_samples.as<uint32_t>();
+    a.rgba = c->r_rgba.as<uint32_t>();
+    a.colored = c->r_misc.as<unsigned long long>();
+    BT_CUDA(c, cudaMemsetAsync(c->r_misc.p, 0, 16, c->stream));
+    const uint32_t n = c->uploaded ? c->samples - c->drawn : 0;
+    if (c->uploaded) {
+        a.xy = xy;
+        a.edge_ids = c->edge_ids.as<uint32_t>();
+        a.segments = c->segments.as<uint32_t>();
+        a.n_segments = n;
+        a.paths = c->paths.as<bt::PathRec>();
+        a.n_paths = c->n_paths;
+        a.density = c->accumulate ? c->norm.as<float>() : nullptr;
+        a.edge_den = static_cast<float>((c->n_paths > 2u ? c->n_paths : 2u) - 1u);   // arrayLength(&edges)
+    }
+    if (n > 0) {
+        const uint64_t cap = c->render_cap;
+        a.bin_blocks = static_cast<uint32_t>((cap + bt::kBinItems - 1) / bt::kBinItems);
+        const size_t hist_n = tiles * a.bin_blocks;
+        if (bt_status s = ensure(c, c->r_seg_count, 8ull * (n + 1))) return s;
+        if (bt_status s = ensure(c, c->r_seg_off, 8ull * (n + 1))) return s;
+        if (bt_status s = ensure(c, c->r_scan64, 8ull * bt::scan_scratch_elems<unsigned long long>(n))) return s;
+        if (bt_status s = ensure(c, c->r_pair_tile, 4 * cap)) return s;
+        if (bt_status s = ensure(c, c->r_pair_seg, 4 * cap)) return s;
+        if (bt_status s = ensure(c, c->r_sorted, 4 * cap)) return s;
+        if (bt_status s = ensure(c, c->r_hist, 4 * hist_n)) return s;
+        if (bt_status s = ensure(c, c->r_hist_off, 4 * (hist_n + 1))) return s;
+        if (bt_status s = ensure(c, c->r_scan32, 4 * bt::scan_scratch_elems<uint32_t>(hist_n))) return s;
+        a.seg_count = c->r_seg_count.as<unsigned long long>();
+        a.seg_off = c->r_seg_off.as<unsigned long long>();
+        a.pair_tile = c->r_pair_tile.as<uint32_t>();
+        a.pair_seg = c->r_pair_seg.as<uint32_t>();
+        a.sorted = c->r_sorted.as<uint32_t>();
+        a.hist = c->r_hist.as<uint32_t>();
+        a.hist_off = c->r_hist_off.as<uint32_t>();
+        a.pair_capacity = cap;
+        a.pair_total = a.seg_off + n;
+        bt::launch_render_bin_count(a, c->stream);
+        bt::exclusive_scan<unsigned long long>(a.seg_count, a.seg_off, n, c->r_scan64.as<unsigned long long>(),
+                                               c->stream);
+        bt::launch_render_bin_emit(a, c->stream);
+        BT_CUDA(c, bt::launch_render_bin_sort(a, c->r_scan32.as<uint32_t>(), c->stream));
+        BT_CUDA(c, cudaMemcpyAsync(c->r_misc.as<unsigned long long>() + 1, a.pair_total, 8, cudaMemcpyDeviceToDevice,
+                                   c->stream));
+    }
+    bt::launch_render_raster(a, c->stream);
+    if (n > 0 && c->opt.endpoint_dots) bt::launch_render_endpoints(a, c->stream);
+    bt::launch_render_resolve(a, c->stream);
+    if (timed) BT_CUDA(c, cudaEventRecord(c->t1, c->stream));
+    BT_CUDA(c, cudaMemcpyAsync(c->h_totals + 2, c->r_misc.p, 16, cudaMemcpyDeviceToHost, c->stream));
+    if (bt_status s = wait(c)) return s;
+    *pairs = c->h_totals[3];
+    *colored = c->h_totals[2];
+    if (*pairs > c->render_cap) return BT_OK;
+    if (rgba) BT_CUDA(c, cudaMemcpyAsync(rgba, c->r_rgba.p, 4 * pixels, cudaMemcpyDeviceToHost, c->stream));
+    return rgba ? wait(c) : BT_OK;
+}
+
+}  // namespace
+
+bt_status bt_render(bt_ctx* c, uint8_t* rgba, size_t rgba_bytes, uint64_t* colored_pixels, float* device_ms) {
+    if (!c) return fail(nullptr, BT_ERR_INVALID, "null context");
+    cudaSetDevice(c->device);
+    const size_t pixels = static_cast<size_t>(c->opt.width) * c->opt.height;
+    if (rgba && rgba_bytes != 4 * pixels) return fail(c, BT_ERR_INVALID, "RGBA buffer must hold 4*width*height bytes");
+    if (bt::render_tile_shift(c->opt.width, c->opt.height) < 0)
+        return fail(c, BT_ERR_INVALID, "frame too large to render (at most 16384 tiles of 64x64 pixels)");
+    const float2* xy = nullptr;
+    if (c->uploaded) {
+        if (bt_status s = current_positions(c, &xy)) return s;
+        if (c->render_cap == 0) c->render_cap = 4ull * (c->samples - c->drawn) + 4096;
+    }
+    if (device_ms) BT_CUDA(c, cudaEventRecord(c->t0, c->stream));
+    uint64_t colored = 0, pairs = 0;
+    if (bt_status s = render_frame(c, xy, device_ms != nullptr, rgba, &colored, &pairs)) return s;
+    if (pairs > c->render_cap) {
+        // The bins were too small: grow them and draw again.
+        if (pairs >= (1ull << 32)) return fail(c, BT_ERR_INVALID, "frame needs more than 2^32 tile bins");
+        c->render_cap = pairs + pairs / 4;
+        if (device_ms) BT_CUDA(c, cudaEventRecord(c->t0, c->stream));
+        if (bt_status s = render_frame(c, xy, device_ms != nullptr, rgba, &colored, &pairs)) return s;
+        if (pairs > c->render_cap) return fail(c, BT_ERR_CUDA, "render bin count changed between passes");
+    }
+    if (device_ms) BT_CUDA(c, cudaEventElapsedTime(device_ms, c->t0, c->t1));
+    if (colored_pixels) *colored_pixels = colored;
     return BT_OK;
 }
 

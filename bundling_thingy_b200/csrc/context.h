@@ -116,6 +116,10 @@ struct bt_ctx {
     bt::DevBuf hist, cell_start, hist_tiles, slot_prefix, prefix_tiles;
     bt::DevBuf counts, himg, vimg, norm, peak;
     bt::DevBuf records, integrals;
+    // bt_render: tile bins, samples, image, and {colored pixels, pairs}.
+    bt::DevBuf r_seg_count, r_seg_off, r_scan64, r_pair_tile, r_pair_seg, r_sorted, r_hist, r_hist_off, r_scan32;
+    bt::DevBuf r_samples, r_rgba, r_misc;
+    uint64_t render_cap = 0;   // (tile, segment) pairs the bin buffers hold
     unsigned long long* h_totals = nullptr;   // pinned
     uint32_t* h_status = nullptr;             // pinned
     size_t device_bytes = 0;

@@ -159,4 +159,50 @@ void launch_positions_from_slots(const uint4* rec, const uint32_t* tag, uint32_t
 void launch_edge_integrals(const PathRec* paths, uint32_t n_paths, const float2* original, const float2* current,
                            double* out, uint32_t* status, cudaStream_t s);
 
+// ---- rendering (render.cu) ----
+// Pairs per block of the stable tile sort; tiles per frame at most (the sort
+// keeps one 4-byte counter per tile in shared memory).
+constexpr uint32_t kBinItems = 16384;
+constexpr uint32_t kMaxRenderTiles = 16384;
+
+struct RenderArgs {
+    const float2* xy;            // current positions, sample order
+    const uint32_t* edge_ids;    // per sample
+    const uint32_t* segments;    // first sample of each segment, draw order
+    uint32_t n_segments;
+    const PathRec* paths;        // endpoint dots
+    uint32_t n_paths;
+    const float* density;        // normalised density, w x h (density colouring)
+    uint32_t w, h;
+    float edge_den;              // max(edges, 2) - 1
+    int color_by_edge, palette, ns;
+    int tile_shift;              // tiles of (1 << tile_shift) pixels square
+    uint32_t tiles_x, tiles_y;
+    unsigned long long* seg_count;   // n_segments: tiles per segment
+    unsigned long long* seg_off;     // n_segments + 1
+    uint32_t* pair_tile;         // pairs, segment order
+    uint32_t* pair_seg;
+    unsigned long long pair_capacity;         // pairs the bin buffers hold
+    const unsigned long long* pair_total;     // device: pairs of this frame (above the
+                                              // capacity: nothing is binned)
+    uint32_t bin_blocks;         // ceil(pair_capacity / kBinItems)
+    uint32_t* hist;              // tiles * bin_blocks
+    uint32_t* hist_off;          // tiles * bin_blocks + 1 (null: no segments)
+    uint32_t* sorted;            // pairs: segment ids, tile-major, draw order
+    uint32_t* samples;           // w * h * ns packed RGB8
+    uint32_t* rgba;              // w * h
+    unsigned long long* colored;
+};
+
+// Tile size for a w x h frame (4, 5 or 6), or -1 when it has too many tiles.
+int render_tile_shift(uint32_t w, uint32_t h);
+void launch_render_bin_count(const RenderArgs& a, cudaStream_t s);
+void launch_render_bin_emit(const RenderArgs& a, cudaStream_t s);
+// Histogram, scan and stable scatter of the pairs by tile; scan_scratch holds
+// scan_scratch_elems<uint32_t>(tiles * bin_blocks) elements.
+cudaError_t launch_render_bin_sort(const RenderArgs& a, uint32_t* scan_scratch, cudaStream_t s);
+void launch_render_raster(const RenderArgs& a, cudaStream_t s);
+void launch_render_endpoints(const RenderArgs& a, cudaStream_t s);
+void launch_render_resolve(const RenderArgs& a, cudaStream_t s);
+
 }  // namespace bt

@@ -45,6 +45,8 @@ enum {
 };
 
 enum { BT_COLOR_BY_DENSITY = 0, BT_COLOR_BY_EDGE_ID = 1 };
+/* --palette (src/palette.rs:13-23); 0 is the reference default. */
+enum { BT_PALETTE_VIRIDIS = 0, BT_PALETTE_CIVIDIS = 1, BT_PALETTE_PLASMA = 2, BT_PALETTE_BATLOW = 3 };
 
 /* Options of Gpu::new (src/main.rs:34-90, src/gpu.rs:60-168). */
 typedef struct bt_options {
@@ -67,7 +69,11 @@ typedef struct bt_options {
     uint32_t search_mode;           /* 0: interior search cells from prefix sums, boundary tested
                                        sample by sample; 1: every candidate tested (same results) */
     uint32_t fine_cells_x;          /* neighbour-search cells per grid cell along x; 0 = fine_cells */
-    uint32_t reserved[5];
+    /* Render options of the reference (src/main.rs:59-82), used by bt_render: */
+    uint32_t palette;               /* --palette: BT_PALETTE_* */
+    uint32_t msaa;                  /* --msaa: 2 or 4 samples per pixel (1 also accepted); 0 = 4 */
+    uint32_t endpoint_dots;         /* --endpoint-dots: dots at the first and last sample of each path */
+    uint32_t reserved[2];
 } bt_options;
 
 typedef struct bt_info {
@@ -166,6 +172,19 @@ bt_status bt_read_neighbors(bt_ctx* ctx, uint32_t* dst, size_t count);
  * (src/main.rs:159-180, src/distortion.rs:172-216); requires
  * evaluate_distortion. size is the canvas size in pixels (gpu::SIZE). */
 bt_status bt_distortion(bt_ctx* ctx, uint32_t size, double* distortion, double* rms_displacement_pixels);
+
+/* Gpu::render + Gpu::readback (src/gpu.rs:572-655) of the headless export:
+ * rasterises the current paths (and the endpoint dots when endpoint_dots is
+ * set) into width x height RGBA8 pixels, rows from the top, with the options'
+ * palette, colouring and msaa; before any upload, the blank frame (the clear
+ * colour) the noisiness report calibrates its background on
+ * (src/main.rs:115-121). rgba (rgba_bytes = 4*width*height) may be NULL;
+ * colored_pixels (may be NULL) receives the number of pixels whose RGB
+ * differs from the clear colour (noisiness::measure, src/noisiness.rs:44-56);
+ * device_ms (may be NULL) the device time of the frame's kernels. The
+ * rasterisation rules are stated in csrc/render.cu; agreement with a
+ * hardware rasteriser is approximate. */
+bt_status bt_render(bt_ctx* ctx, uint8_t* rgba, size_t rgba_bytes, uint64_t* colored_pixels, float* device_ms);
 
 /* Per-stage device milliseconds of the last upload/iteration, as the
  * reference's GpuTimings (src/profiling.rs:35-136). names/ms hold `capacity`

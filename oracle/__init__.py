@@ -95,6 +95,11 @@ def lib():
         L.or_neighbor_mean_sample.restype = ctypes.c_size_t
         L.or_squared_integral.argtypes = [_f32p, ctypes.c_size_t, _f32p, ctypes.c_size_t, _f64p]
         L.or_distortion.argtypes = [_u32p, ctypes.c_uint32, _f32p, _f32p, ctypes.c_uint32, _f64p, _f64p]
+        L.or_half_round.argtypes = [ctypes.c_float]
+        L.or_half_round.restype = ctypes.c_float
+        L.or_render.argtypes = [_f32p, _u32p, _u32p, ctypes.c_uint32, ctypes.c_uint32, _f32p, ctypes.c_uint32,
+                                ctypes.c_uint32, ctypes.c_int, ctypes.c_int, ctypes.c_int, _u32p, ctypes.c_uint32,
+                                ctypes.c_int, _u8p, ctypes.POINTER(ctypes.c_uint64)]
         _lib = L
     return _lib
 
@@ -228,6 +233,29 @@ def distortion(paths, original_xy, current_xy, size):
     if rc:
         raise OracleError(rc, "distortion failed")
     return d.value, r.value
+
+
+def half_round(v: float) -> float:
+    return lib().or_half_round(v)
+
+
+def render(xy, edge_ids, segments, n_edges, density, w, h, color_by_edge=False, palette=0, msaa=4,
+           paths=None, endpoint_dots=False):
+    """Path rasterisation (render.cpp): (RGBA8 array h x w x 4, colored pixel count).
+    paths: n x 3 u32 (point offset, segment offset, count), for the endpoint dots."""
+    xy = np.ascontiguousarray(xy, np.float32)
+    paths = np.ascontiguousarray(paths if paths is not None else np.zeros((0, 3)), np.uint32)
+    edge_ids = np.ascontiguousarray(edge_ids, np.uint32)
+    segments = np.ascontiguousarray(segments, np.uint32)
+    density = np.ascontiguousarray(density if density is not None else np.zeros(w * h), np.float32)
+    out = np.zeros((h, w, 4), np.uint8)
+    colored = ctypes.c_uint64()
+    rc = lib().or_render(_p(xy, _f32p), _p(edge_ids, _u32p), _p(segments, _u32p), segments.size, n_edges,
+                         _p(density, _f32p), w, h, int(bool(color_by_edge)), palette, msaa, _p(paths, _u32p),
+                         paths.size // 3, int(bool(endpoint_dots)), _p(out, _u8p), ctypes.byref(colored))
+    if rc:
+        raise OracleError(rc, "render failed")
+    return out, colored.value
 
 
 @dataclass

@@ -104,6 +104,17 @@ int or_squared_integral(const float* original, size_t n_original, const float* c
 int or_distortion(const uint32_t* paths, uint32_t n_paths, const float* original_xy,
                   const float* current_xy, uint32_t size, double* distortion, double* rms_pixels);
 
+/* Path rasterisation and the noisiness count (render.cpp): RGBA8 of w*h
+ * pixels and the number of pixels whose RGB differs from the background.
+ * palette 0 viridis, 1 cividis, 2 plasma, 3 batlow; msaa 1, 2 or 4; paths
+ * (3 u32 per edge: point offset, segment offset, count) give the endpoint
+ * dots when endpoint_dots is set. Returns 0 on success. */
+float or_half_round(float v);   /* f32 -> f16 (nearest even) -> f32 */
+int or_render(const float* xy, const uint32_t* edge_ids, const uint32_t* segments, uint32_t n_segments,
+              uint32_t n_edges, const float* density, uint32_t w, uint32_t h, int color_by_edge, int palette,
+              int msaa, const uint32_t* paths, uint32_t n_paths, int endpoint_dots, uint8_t* rgba,
+              uint64_t* colored);
+
 #ifdef __cplusplus
 }
 #endif
