@@ -1180,6 +1180,10 @@ bt_status bt_render(bt_ctx* c, uint8_t* rgba, size_t rgba_bytes, uint64_t* color
         if (bt_status s = current_positions(c, &xy)) return s;
         if (c->render_cap == 0) c->render_cap = 4ull * (c->samples - c->drawn) + 4096;
     }
+    if (device_ms && !c->t0) {
+        BT_CUDA(c, cudaEventCreate(&c->t0));
+        BT_CUDA(c, cudaEventCreate(&c->t1));
+    }
     if (device_ms) BT_CUDA(c, cudaEventRecord(c->t0, c->stream));
     uint64_t colored = 0, pairs = 0;
     if (bt_status s = render_frame(c, xy, device_ms != nullptr, rgba, &colored, &pairs)) return s;
