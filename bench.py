@@ -51,7 +51,9 @@ def parse_args():
     p.add_argument("--e2e-jobs", type=int, default=3)
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU work of the baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--workload", choices=["large", "batched", "served"], default="large")
+    p.add_argument("--workload", choices=["large", "batched", "served", "render"], default="large")
+    p.add_argument("--render-iterations", type=int, default=30,
+                   help="render workload: mean updates before the frames are drawn")
     p.add_argument("--graphs", type=int, default=256, help="batched workload: number of graphs")
     p.add_argument("--batch-iterations", type=int, default=10)
     p.add_argument("--requests", type=int, default=1000, help="served workload: requests per rank")
@@ -382,6 +384,78 @@ def run_ours(args, ranks: Ranks):
         print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------- render
+def run_render(args, ranks: Ranks):
+    """Frames of the large workload's bundled geometry (bt_render: tile
+    binning, ordered blending, endpoint-free density colouring at 4x MSAA,
+    the reference's render defaults), against the oracle's rasteriser on one
+    host thread."""
+    import bundling_thingy_b200 as bt
+
+    w = workload(args.edges)
+    device = ranks.local
+    opts = bt.Options(width=w.width, height=w.height, neighbor_radius=w.radius, sample_spacing=w.spacing,
+                      blur_sigma=w.sigma, device=device)
+    gpu = bt.Gpu(opts)
+    n = gpu.upload((w.xy, w.starts))
+    gpu.iterate(args.render_iterations)
+    segments = gpu.info().segments
+    for _ in range(max(args.warmup, 3)):
+        gpu.render(pixels=False)
+    sampler = ClockSampler(device)
+    sampler.start()
+    ranks.barrier()
+    frame_ms = [gpu.render(pixels=False).device_ms for _ in range(args.steps)]
+    ranks.barrier()
+    clocks = sampler.stop()
+    ms = ranks.max(statistics.median(frame_ms))
+    value = ranks.sum(1.0) / (ms / 1e3)
+    # End to end: the frame and its RGBA8 readback into pinned host memory.
+    import torch
+
+    rgba = torch.empty(w.width * w.height * 4, dtype=torch.uint8, pin_memory=True).numpy().reshape(
+        w.height, w.width, 4)
+    walls = []
+    for i in range(args.steps + 1):
+        t0 = time.perf_counter()
+        f = gpu.render(out=rgba)
+        if i:
+            walls.append(time.perf_counter() - t0)
+    wall = ranks.max(statistics.median(walls))
+    colored = f.colored_pixels
+    cpu = None
+    if ranks.rank == 0 and ranks.world == 1 and not args.no_cpu_baseline:
+        import oracle as O
+
+        xy, ids = gpu.read_points()
+        seg, paths, dens = gpu.read_segments(), gpu.read_paths(), gpu.read_density()
+        t0 = time.perf_counter()
+        _, c_colored = O.render(xy, ids, seg, paths.shape[0], dens, w.width, w.height)
+        t_cpu = time.perf_counter() - t0
+        assert c_colored == colored
+        cpu = {"value": 1.0 / t_cpu, "unit": "frames/s", "cores": 1, "kind": "port",
+               "sample": f"one whole frame ({segments} segments, {w.width}x{w.height}, 4x MSAA) by the oracle's "
+                         f"sequential rasteriser; same coloured-pixel count"}
+    gpu.close()
+    line = {
+        "metric": "frames/s", "value": value, "unit": "frames/s", "n_gpus": ranks.world, "steps": args.steps,
+        "warmup": max(args.warmup, 3), "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8/i64",
+        "data": "synthetic (seeded random-walk polylines)",
+        "config": {"workload": (f"render: large ({n} samples, {segments} segments) after "
+                                f"{args.render_iterations} iterations, {w.width}x{w.height}, 4x MSAA, density "
+                                "colour, no endpoint dots"),
+                   "colored_pixels": colored, "l2": "frame state (64 MB of samples) rewritten each frame"},
+        "e2e": {"value": 1.0 / wall, "unit": "frames/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": w.width * w.height * 4 + 16,
+                "step": "bt_render with the RGBA8 readback into pinned host memory"},
+        "clocks": clocks,
+        "cpu_baseline": cpu,
+    }
+    if ranks.rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 # ---------------------------------------------------------------- batched
 def run_batched(args, ranks: Ranks):
     """256 independent graphs (edges log-uniform 200-20,000, grids 256/512/1024),
@@ -694,6 +768,8 @@ def main():
             run_batched(args, ranks)
         elif args.workload == "served":
             run_served(args, ranks)
+        elif args.workload == "render":
+            run_render(args, ranks)
         else:
             run_ours(args, ranks)
     finally:

@@ -1175,16 +1175,16 @@ bt_status bt_render(bt_ctx* c, uint8_t* rgba, size_t rgba_bytes, uint64_t* color
     if (rgba && rgba_bytes != 4 * pixels) return fail(c, BT_ERR_INVALID, "RGBA buffer must hold 4*width*height bytes");
     if (bt::render_tile_shift(c->opt.width, c->opt.height) < 0)
         return fail(c, BT_ERR_INVALID, "frame too large to render (at most 16384 tiles of 64x64 pixels)");
-    const float2* xy = nullptr;
-    if (c->uploaded) {
-        if (bt_status s = current_positions(c, &xy)) return s;
-        if (c->render_cap == 0) c->render_cap = 4ull * (c->samples - c->drawn) + 4096;
-    }
     if (device_ms && !c->t0) {
         BT_CUDA(c, cudaEventCreate(&c->t0));
         BT_CUDA(c, cudaEventCreate(&c->t1));
     }
     if (device_ms) BT_CUDA(c, cudaEventRecord(c->t0, c->stream));
+    const float2* xy = nullptr;
+    if (c->uploaded) {
+        if (bt_status s = current_positions(c, &xy)) return s;
+        if (c->render_cap == 0) c->render_cap = 4ull * (c->samples - c->drawn) + 4096;
+    }
     uint64_t colored = 0, pairs = 0;
     if (bt_status s = render_frame(c, xy, device_ms != nullptr, rgba, &colored, &pairs)) return s;
     if (pairs > c->render_cap) {

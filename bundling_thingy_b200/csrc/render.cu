@@ -93,9 +93,15 @@ struct TriSetup {
 struct SegSetup {
     TriSetup t[2];
     int x0, y0, x1, y1;
+    float col[3];     // palette colour (edge-id colouring; set by the raster kernel)
     uint32_t first;
-    uint32_t valid;   // bit k: triangle k has nonzero area
+    uint32_t valid;   // bit k: triangle k has nonzero area; kSmall: 32-bit edge functions suffice
 };
+
+// Set when the snapped corners span less than 64 pixels in x and in y: every
+// edge function over the segment's pixel box then stays below 2^30 in
+// magnitude and is evaluated exactly in 32 bits.
+constexpr uint32_t kSmall = 4u;
 
 __device__ __forceinline__ long long edge_fn(int ax, int ay, int dx, int dy, long long px, long long py) {
     return static_cast<long long>(dx) * (py - ay) - static_cast<long long>(dy) * (px - ax);
@@ -187,16 +193,16 @@ __device__ __forceinline__ void seg_setup(const RenderArgs& a, uint32_t s, SegSe
         }
     }
     if (!g->valid) return;
+    if (maxx - minx < (1 << 14) && maxy - miny < (1 << 14)) g->valid |= kSmall;
     g->x0 = max(0, minx >> 8);
     g->x1 = min(static_cast<int>(a.w) - 1, maxx >> 8);
     g->y0 = max(0, miny >> 8);
     g->y1 = min(static_cast<int>(a.h) - 1, maxy >> 8);
 }
 
-// fs_main's palette position for pixel (x, y) of a segment starting at
-// sample `first`.
-__device__ __forceinline__ float value_at(const RenderArgs& a, int x, int y, uint32_t first) {
-    if (a.color_by_edge) return __fdiv_rn(static_cast<float>(a.edge_ids[first]), a.edge_den);
+// fs_main's palette position of the density texture at pixel (x, y): the
+// same for every segment drawn there.
+__device__ __forceinline__ float pixel_value(const RenderArgs& a, int x, int y) {
     const float u = __fdiv_rn(__fadd_rn(static_cast<float>(x), 0.5f), static_cast<float>(a.w));
     const float v = __fdiv_rn(__fadd_rn(static_cast<float>(y), 0.5f), static_cast<float>(a.h));
     const float tx = __fmul_rn(u, static_cast<float>(a.w - 1u)), ty = __fmul_rn(v, static_cast<float>(a.h - 1u));
@@ -215,18 +221,36 @@ __device__ __forceinline__ float value_at(const RenderArgs& a, int x, int y, uin
     return fminf(fmaxf(value, 0.0f), 1.0f);
 }
 
+// fs_main's palette position of a segment starting at sample `first` under
+// edge-id colouring.
+__device__ __forceinline__ float edge_value(const RenderArgs& a, uint32_t first) {
+    return __fdiv_rn(static_cast<float>(a.edge_ids[first]), a.edge_den);
+}
+
+// The 16-stop palette lerp of fs_main.
+__device__ __forceinline__ void palette_color(const float (*pal)[3], float value, float col[3]) {
+    const float stop = __fmul_rn(value, 15.0f);
+    uint32_t idx = static_cast<uint32_t>(stop);
+    if (idx > 14u) idx = 14u;
+    const float f = __fsub_rn(stop, static_cast<float>(idx));
+#pragma unroll
+    for (int ch = 0; ch < 3; ++ch)
+        col[ch] = __fadd_rn(__fmul_rn(pal[idx][ch], __fsub_rn(1.0f, f)), __fmul_rn(pal[idx + 1][ch], f));
+}
+
 __device__ __forceinline__ uint32_t to_u8(float r) {
     return static_cast<uint32_t>(fminf(fmaxf(rintf(__fmul_rn(r, 255.0f)), 0.0f), 255.0f));
 }
 
-// One blend of colour col (alpha 0.1) into a packed RGB8 sample.
-__device__ __forceinline__ uint32_t blend(uint32_t packed, const float col[3]) {
+// One blend (alpha 0.1) into a packed RGB8 sample: src = col * 0.1 per
+// channel, unorm[c] = c / 255 (IEEE quotients, tabulated).
+__device__ __forceinline__ uint32_t blend(uint32_t packed, const float src[3], const float* unorm) {
     const float keep = __fsub_rn(1.0f, 0.1f);
     uint32_t out = 0;
 #pragma unroll
     for (int ch = 0; ch < 3; ++ch) {
-        const float dst = __fdiv_rn(static_cast<float>((packed >> (8 * ch)) & 0xFFu), 255.0f);
-        out |= to_u8(__fadd_rn(__fmul_rn(col[ch], 0.1f), __fmul_rn(dst, keep))) << (8 * ch);
+        const float dst = unorm[(packed >> (8 * ch)) & 0xFFu];
+        out |= to_u8(__fadd_rn(src[ch], __fmul_rn(dst, keep))) << (8 * ch);
     }
     return out;
 }
@@ -321,28 +345,74 @@ __global__ void __launch_bounds__(256) bin_rank_kernel(RenderArgs a) {
 
 constexpr int kChunk = 256;
 
-// One CTA per tile of T x T pixels (T = 16, 32 or 64 for PPT = 1, 4, 16);
-// thread t owns the PPT pixels (t % T, t / T + k * 256 / T) of the tile and
-// keeps their samples in registers while it walks the tile's segments in
-// draw order, 256 segment setups at a time.
-template <int PPT>
+// Covering triangles of sample (sx, sy) relative to the pixel box: 0, 1 or 2
+// (both only for a folded, degenerate quad; each blends once). Small
+// segments use exact 32-bit edge functions, others 64-bit ones.
+__device__ __forceinline__ int covering(const SegSetup& g, int sx, int sy) {
+    int n = 0;
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+        if (!(g.valid & (1u << t))) continue;
+        bool in = true;
+        if (g.valid & kSmall) {
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                const int dx = g.t[t].dx[j], dy = g.t[t].dy[j];
+                const int f = dx * (sy - g.t[t].ay[j]) - dy * (sx - g.t[t].ax[j]);
+                const bool tl = dy > 0 || (dy == 0 && dx < 0);
+                in &= f > 0 || (f == 0 && tl);
+            }
+        } else {
+            in = inside(g.t[t], sx, sy);
+        }
+        n += in;
+    }
+    return n;
+}
+
+// One CTA per tile of T x T pixels (T = 16, 32 or 64). Warp w owns the band
+// of T / 8 rows starting at row w * T / 8; its lanes own the band's pixels
+// (T = 16: lane -> column lane % 16, row lane / 16; T >= 32: columns
+// lane + 32 c, every row of the band) and keep their samples in registers.
+// The CTA sets up 256 segments of the tile's list at a time; each warp
+// walks, in draw order, those whose box meets its band (a ballot per 32).
+template <int T>
 __global__ void __launch_bounds__(256) raster_kernel(RenderArgs a) {
-    constexpr int T = PPT == 1 ? 16 : PPT == 4 ? 32 : 64;
-    constexpr int kRows = 256 / T;
+    constexpr int kRows = T / 8;
+    constexpr int kCols = T >= 32 ? T / 32 : 1;
+    constexpr int PPT = T >= 32 ? kRows * kCols : 1;
+    constexpr bool kCacheColour = PPT <= 4;
     __shared__ SegSetup segs[kChunk];
     __shared__ float pal[16][3];
+    __shared__ float unorm[256];
     if (threadIdx.x < 48) pal[threadIdx.x / 3][threadIdx.x % 3] = kPalette[a.palette][threadIdx.x / 3][threadIdx.x % 3];
+    unorm[threadIdx.x] = __fdiv_rn(static_cast<float>(threadIdx.x), 255.0f);
+    __syncthreads();
+    const int lane = static_cast<int>(threadIdx.x) & 31, warp = static_cast<int>(threadIdx.x) >> 5;
     const uint32_t tile = blockIdx.x;
     const int tx = static_cast<int>(tile % a.tiles_x), ty = static_cast<int>(tile / a.tiles_x);
-    const int px = tx * T + static_cast<int>(threadIdx.x) % T;
-    int py[PPT];
+    const int band0 = ty * T + warp * kRows, band1 = band0 + kRows - 1;
+    int px[PPT], py[PPT];
     uint32_t samp[PPT][4];
+    float pcol[kCacheColour ? PPT : 1][3];
     const uint32_t bg = clear_color();
 #pragma unroll
     for (int k = 0; k < PPT; ++k) {
-        py[k] = ty * T + static_cast<int>(threadIdx.x) / T + k * kRows;
+        if (T == 16) {
+            px[k] = tx * T + (lane & 15);
+            py[k] = band0 + (lane >> 4);
+        } else {
+            px[k] = tx * T + lane + 32 * (k % kCols);
+            py[k] = band0 + k / kCols;
+        }
 #pragma unroll
         for (int q = 0; q < 4; ++q) samp[k][q] = bg;
+        if (kCacheColour && !a.color_by_edge && px[k] < static_cast<int>(a.w) && py[k] < static_cast<int>(a.h)) {
+            float c[3];
+            palette_color(pal, pixel_value(a, px[k], py[k]), c);
+#pragma unroll
+            for (int ch = 0; ch < 3; ++ch) pcol[kCacheColour ? k : 0][ch] = __fmul_rn(c[ch], 0.1f);
+        }
     }
     size_t begin = 0, end = 0;
     if (a.hist_off) {
@@ -352,56 +422,65 @@ __global__ void __launch_bounds__(256) raster_kernel(RenderArgs a) {
     for (size_t chunk = begin; chunk < end; chunk += kChunk) {
         const int n = static_cast<int>(min(static_cast<size_t>(kChunk), end - chunk));
         __syncthreads();
-        if (static_cast<int>(threadIdx.x) < n) seg_setup(a, a.sorted[chunk + threadIdx.x], &segs[threadIdx.x]);
+        if (static_cast<int>(threadIdx.x) < n) {
+            SegSetup& g = segs[threadIdx.x];
+            seg_setup(a, a.sorted[chunk + threadIdx.x], &g);
+            if (a.color_by_edge) {
+                palette_color(pal, edge_value(a, g.first), g.col);
+#pragma unroll
+                for (int ch = 0; ch < 3; ++ch) g.col[ch] = __fmul_rn(g.col[ch], 0.1f);
+            }
+        }
         __syncthreads();
-        for (int e = 0; e < n; ++e) {
-            const SegSetup& g = segs[e];
-            if (px < g.x0 || px > g.x1) continue;
+        for (int base = 0; base < n; base += 32) {
+            const int e0 = base + lane;
+            const bool hit = e0 < n && segs[e0].y0 <= band1 && segs[e0].y1 >= band0;
+            unsigned mask = __ballot_sync(0xFFFFFFFFu, hit);
+            while (mask) {
+                const int e = base + __ffs(mask) - 1;
+                mask &= mask - 1;
+                const SegSetup& g = segs[e];
 #pragma unroll
-            for (int k = 0; k < PPT; ++k) {
-                if (py[k] < g.y0 || py[k] > g.y1) continue;
-                // Covering triangles per sample (both only for a degenerate
-                // quad; each blends once).
-                int cover[4] = {0, 0, 0, 0};
-                bool any = false;
-#pragma unroll
-                for (int t = 0; t < 2; ++t) {
-                    if (!(g.valid & (1u << t))) continue;
+                for (int k = 0; k < PPT; ++k) {
+                    if (px[k] < g.x0 || px[k] > g.x1 || py[k] < g.y0 || py[k] > g.y1) continue;
+                    int cover[4];
+                    bool any = false;
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
+                        cover[q] = 0;
                         if (q < a.ns) {
                             int ox, oy;
                             sample_offset(a.ns, q, &ox, &oy);
-                            if (inside(g.t[t], static_cast<long long>(px) * 256 + ox,
-                                       static_cast<long long>(py[k]) * 256 + oy)) {
-                                ++cover[q];
-                                any = true;
-                            }
+                            cover[q] = covering(g, px[k] * 256 + ox, py[k] * 256 + oy);
+                            any |= cover[q] != 0;
                         }
                     }
-                }
-                if (!any) continue;
-                const float value = value_at(a, px, py[k], g.first);
-                const float stop = __fmul_rn(value, 15.0f);
-                uint32_t idx = static_cast<uint32_t>(stop);
-                if (idx > 14u) idx = 14u;
-                const float f = __fsub_rn(stop, static_cast<float>(idx));
-                float col[3];
+                    if (!any) continue;
+                    float src[3];
+                    if (a.color_by_edge) {
 #pragma unroll
-                for (int ch = 0; ch < 3; ++ch)
-                    col[ch] = __fadd_rn(__fmul_rn(pal[idx][ch], __fsub_rn(1.0f, f)), __fmul_rn(pal[idx + 1][ch], f));
+                        for (int ch = 0; ch < 3; ++ch) src[ch] = g.col[ch];
+                    } else if (kCacheColour) {
 #pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    if (cover[q] > 0) samp[k][q] = blend(samp[k][q], col);
-                    if (cover[q] > 1) samp[k][q] = blend(samp[k][q], col);
+                        for (int ch = 0; ch < 3; ++ch) src[ch] = pcol[kCacheColour ? k : 0][ch];
+                    } else {
+                        palette_color(pal, pixel_value(a, px[k], py[k]), src);
+#pragma unroll
+                        for (int ch = 0; ch < 3; ++ch) src[ch] = __fmul_rn(src[ch], 0.1f);
+                    }
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        if (cover[q] > 0) samp[k][q] = blend(samp[k][q], src, unorm);
+                        if (cover[q] > 1) samp[k][q] = blend(samp[k][q], src, unorm);
+                    }
                 }
             }
         }
     }
 #pragma unroll
     for (int k = 0; k < PPT; ++k) {
-        if (px >= static_cast<int>(a.w) || py[k] >= static_cast<int>(a.h)) continue;
-        const size_t base = (static_cast<size_t>(py[k]) * a.w + px) * a.ns;
+        if (px[k] >= static_cast<int>(a.w) || py[k] >= static_cast<int>(a.h)) continue;
+        const size_t base = (static_cast<size_t>(py[k]) * a.w + px[k]) * a.ns;
 #pragma unroll
         for (int q = 0; q < 4; ++q)
             if (q < a.ns) a.samples[base + q] = samp[k][q];
@@ -533,9 +612,9 @@ cudaError_t launch_render_bin_sort(const RenderArgs& a, uint32_t* scan_scratch, 
 
 void launch_render_raster(const RenderArgs& a, cudaStream_t s) {
     const unsigned tiles = a.tiles_x * a.tiles_y;
-    if (a.tile_shift == 4) raster_kernel<1><<<tiles, 256, 0, s>>>(a);
-    else if (a.tile_shift == 5) raster_kernel<4><<<tiles, 256, 0, s>>>(a);
-    else raster_kernel<16><<<tiles, 256, 0, s>>>(a);
+    if (a.tile_shift == 4) raster_kernel<16><<<tiles, 256, 0, s>>>(a);
+    else if (a.tile_shift == 5) raster_kernel<32><<<tiles, 256, 0, s>>>(a);
+    else raster_kernel<64><<<tiles, 256, 0, s>>>(a);
 }
 
 void launch_render_endpoints(const RenderArgs& a, cudaStream_t s) {

@@ -6,6 +6,8 @@ blends in draw order. The frame (RGBA8) and its coloured-pixel count must
 match bit for bit, for every palette, colouring, sample count and tile size,
 before and after iterations.
 """
+import json
+
 import numpy as np
 import pytest
 
@@ -114,3 +116,38 @@ def test_render_count_only_and_bad_buffer():
     assert full.device_ms > 0
     with pytest.raises(ValueError):
         gpu.render(out=np.zeros((10, 10, 4), np.uint8))
+
+
+def test_headless_run_writes_images_and_reports(oracle, tmp_path, capsys):
+    # src/main.rs:104-221: blank-frame calibration, original.png, one image
+    # per iteration, noisiness.json and distortion.json.
+    from bundling_thingy_b200 import report
+
+    w = synthetic.small()
+    trl = tmp_path / "g.trl"
+    synthetic.write_trl(trl, w.xy, w.starts)
+    o = bt.Options(width=w.width, height=w.height, sample_spacing=w.spacing, blur_sigma=w.sigma,
+                   blur_shrink=w.shrink, color_by=bt.COLOR_BY_EDGE_ID)
+    out_dir = tmp_path / "out"
+    r = report.headless(trl, out_dir, neighbor_radius=w.radius, iterations=2, options=o, evaluate_noisiness=True,
+                        evaluate_distortion=True)
+    lines = capsys.readouterr().out.splitlines()
+    assert lines[0].startswith("noisiness original.png: ") and lines[0].endswith("change +0.000000")
+    assert lines[1] == f"wrote {out_dir / 'original.png'}"
+    assert lines[2] == "original.png distortion=0 rms_displacement_pixels=0"
+    assert lines[3].startswith("noisiness iteration-01.png: ")
+    assert lines[4] == f"wrote {out_dir / 'iteration-01.png'}"
+    assert lines[5].startswith("iteration-01.png distortion=")
+    assert lines[-1] == f"rendered {r['samples']} samples to {out_dir}"
+    noise = json.loads((out_dir / "noisiness.json").read_text())
+    assert noise == r["noisiness"] and noise["render"]["background_rgb"] == [6, 6, 9]
+    assert [i["file"] for i in noise["images"]] == ["original.png", "iteration-01.png", "iteration-02.png"]
+    assert json.loads((out_dir / "distortion.json").read_text()) == r["distortion"]
+    # The last image against a fresh run of the same graph and the oracle.
+    o2 = bt.Options(**{**o.__dict__, "neighbor_radius": w.radius})
+    gpu = bt.Gpu(o2)
+    gpu.upload(bt.Graph.load(trl))
+    gpu.iterate(2)
+    frame = check(oracle, gpu, o2)
+    np.testing.assert_array_equal(report.read_png(out_dir / "iteration-02.png"), frame.rgba)
+    assert noise["images"][-1]["colored_pixels"] == frame.colored_pixels
