@@ -407,17 +407,23 @@ __global__ void __launch_bounds__(256) raster_kernel(RenderArgs a) {
         }
 #pragma unroll
         for (int q = 0; q < 4; ++q) samp[k][q] = bg;
-        if (kCacheColour && !a.color_by_edge && px[k] < static_cast<int>(a.w) && py[k] < static_cast<int>(a.h)) {
-            float c[3];
-            palette_color(pal, pixel_value(a, px[k], py[k]), c);
-#pragma unroll
-            for (int ch = 0; ch < 3; ++ch) pcol[kCacheColour ? k : 0][ch] = __fmul_rn(c[ch], 0.1f);
-        }
     }
     size_t begin = 0, end = 0;
     if (a.hist_off) {
         begin = a.hist_off[static_cast<size_t>(tile) * a.bin_blocks];
         end = a.hist_off[static_cast<size_t>(tile + 1) * a.bin_blocks];
+    }
+    // Density colour of each owned pixel, once (only a tile with segments
+    // reads the density map, which exists once a graph is uploaded).
+    if (kCacheColour && !a.color_by_edge && begin < end && a.density) {
+#pragma unroll
+        for (int k = 0; k < PPT; ++k) {
+            if (px[k] >= static_cast<int>(a.w) || py[k] >= static_cast<int>(a.h)) continue;
+            float c[3];
+            palette_color(pal, pixel_value(a, px[k], py[k]), c);
+#pragma unroll
+            for (int ch = 0; ch < 3; ++ch) pcol[kCacheColour ? k : 0][ch] = __fmul_rn(c[ch], 0.1f);
+        }
     }
     for (size_t chunk = begin; chunk < end; chunk += kChunk) {
         const int n = static_cast<int>(min(static_cast<size_t>(kChunk), end - chunk));
