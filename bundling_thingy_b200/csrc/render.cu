@@ -155,6 +155,22 @@ __device__ __forceinline__ void set_edges(const int* vx, const int* vy, const in
     }
 }
 
+// The snapped corners of the quad of the segment starting at sample i
+// (vs_main + the viewport); false when one is too far off screen.
+__device__ __forceinline__ bool quad_corners(const RenderArgs& a, uint32_t i, int* vx, int* vy) {
+    const float2 p = a.xy[i], q = a.xy[i + 1];
+    const float dx = __fsub_rn(q.x, p.x), dy = __fsub_rn(q.y, p.y);
+    const float len = __fsqrt_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)));
+    const float k = __fdiv_rn(0.001f, fmaxf(len, 1e-10f));
+    const float nx = __fmul_rn(-dy, k), ny = __fmul_rn(dx, k);
+    const float cx[4] = {__fadd_rn(p.x, nx), __fsub_rn(p.x, nx), __fadd_rn(q.x, nx), __fsub_rn(q.x, nx)};
+    const float cy[4] = {__fadd_rn(p.y, ny), __fsub_rn(p.y, ny), __fadd_rn(q.y, ny), __fsub_rn(q.y, ny)};
+    bool ok = true;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) ok &= snap(cx[c], cy[c], a.w, a.h, &vx[c], &vy[c]);
+    return ok;
+}
+
 // Setup of segment s (vs_main + the viewport).
 __device__ __forceinline__ void seg_setup(const RenderArgs& a, uint32_t s, SegSetup* g) {
     const uint32_t i = a.segments[s];
@@ -164,18 +180,8 @@ __device__ __forceinline__ void seg_setup(const RenderArgs& a, uint32_t s, SegSe
     g->x1 = 0;
     g->y0 = 1;
     g->y1 = 0;
-    const float2 p = a.xy[i], q = a.xy[i + 1];
-    const float dx = __fsub_rn(q.x, p.x), dy = __fsub_rn(q.y, p.y);
-    const float len = __fsqrt_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)));
-    const float k = __fdiv_rn(0.001f, fmaxf(len, 1e-10f));
-    const float nx = __fmul_rn(-dy, k), ny = __fmul_rn(dx, k);
-    const float cx[4] = {__fadd_rn(p.x, nx), __fsub_rn(p.x, nx), __fadd_rn(q.x, nx), __fsub_rn(q.x, nx)};
-    const float cy[4] = {__fadd_rn(p.y, ny), __fsub_rn(p.y, ny), __fadd_rn(q.y, ny), __fsub_rn(q.y, ny)};
     int vx[4], vy[4];
-    bool ok = true;
-#pragma unroll
-    for (int c = 0; c < 4; ++c) ok &= snap(cx[c], cy[c], a.w, a.h, &vx[c], &vy[c]);
-    if (!ok) return;
+    if (!quad_corners(a, i, vx, vy)) return;
     int minx = INT_MAX, maxx = INT_MIN, miny = INT_MAX, maxy = INT_MIN;
 #pragma unroll
     for (int t = 0; t < 2; ++t) {
@@ -343,46 +349,128 @@ __global__ void __launch_bounds__(256) bin_rank_kernel(RenderArgs a) {
 
 // ---------------------------------------------------------------- raster
 
-constexpr int kChunk = 256;
+constexpr int kChunk = 128;
+constexpr uint32_t kSlow = 1u;
 
-// Covering triangles of sample (sx, sy) relative to the pixel box: 0, 1 or 2
-// (both only for a folded, degenerate quad; each blends once). Small
-// segments use exact 32-bit edge functions, others 64-bit ones.
-__device__ __forceinline__ int covering(const SegSetup& g, int sx, int sy) {
-    int n = 0;
+// A segment as the raster kernel tests it. For a small segment (kSmall) the
+// six edge functions of its two triangles are kept relative to the origin
+// (X0, Y0) = 256 * (x0, y0) of its pixel box, with the top-left rule folded
+// in: for edge j, f_j(sx, sy) - bias_j = E_j + dx_j * (sy - Y0) - dy_j * (sx - X0),
+// bias_j = 0 on a top-left edge and 1 otherwise, so a sample is inside
+// triangle t when the three values of its edges are all >= 0 (their OR has
+// no sign bit). K_j[q] = dx_j * oy_q - dy_j * ox_q adds sample q's offset.
+// A triangle of zero area has E = -1, dx = dy = K = 0 (never inside). Other
+// segments (kSlow) are tested in 64 bits from their setup.
+struct __align__(16) FastSeg {
+    int4 edge[6];     // dx, dy, E, 0
+    int4 k[6];        // K per sample
+    int4 box;         // x0, y0, x1, y1
+    float4 src;       // edge-id colour * 0.1
+    uint32_t seg, flags, pad0, pad1;
+};
+
+__device__ __forceinline__ void fast_setup(const RenderArgs& a, uint32_t s, const float (*pal)[3], FastSeg* f) {
+    int vx[4], vy[4];
+    const uint32_t first = a.segments[s];
+    f->seg = s;
+    // The segment is in this tile's list, so its quad is on screen and has a
+    // triangle of nonzero area.
+    quad_corners(a, first, vx, vy);
+    int order[2][3];
+    bool valid[2];
+    int minx = INT_MAX, maxx = INT_MIN, miny = INT_MAX, maxy = INT_MIN;
 #pragma unroll
     for (int t = 0; t < 2; ++t) {
-        if (!(g.valid & (1u << t))) continue;
-        bool in = true;
-        if (g.valid & kSmall) {
+        order[t][0] = t == 0 ? 0 : 2;
+        order[t][1] = 1;
+        order[t][2] = t == 0 ? 2 : 3;
+        long long area;
+        valid[t] = orient(vx, vy, order[t], &area);
+        if (!valid[t]) continue;
 #pragma unroll
-            for (int j = 0; j < 3; ++j) {
-                const int dx = g.t[t].dx[j], dy = g.t[t].dy[j];
-                const int f = dx * (sy - g.t[t].ay[j]) - dy * (sx - g.t[t].ax[j]);
-                const bool tl = dy > 0 || (dy == 0 && dx < 0);
-                in &= f > 0 || (f == 0 && tl);
-            }
-        } else {
-            in = inside(g.t[t], sx, sy);
+        for (int j = 0; j < 3; ++j) {
+            minx = min(minx, vx[order[t][j]]);
+            maxx = max(maxx, vx[order[t][j]]);
+            miny = min(miny, vy[order[t][j]]);
+            maxy = max(maxy, vy[order[t][j]]);
         }
-        n += in;
     }
-    return n;
+    const int x0 = max(0, minx >> 8), y0 = max(0, miny >> 8);
+    f->box = make_int4(x0, y0, min(static_cast<int>(a.w) - 1, maxx >> 8), min(static_cast<int>(a.h) - 1, maxy >> 8));
+    const bool small = maxx - minx < (1 << 14) && maxy - miny < (1 << 14);
+    f->flags = small ? 0u : kSlow;
+    float col[3] = {0.0f, 0.0f, 0.0f};
+    if (a.color_by_edge) {
+        palette_color(pal, edge_value(a, first), col);
+#pragma unroll
+        for (int ch = 0; ch < 3; ++ch) col[ch] = __fmul_rn(col[ch], 0.1f);
+    }
+    f->src = make_float4(col[0], col[1], col[2], 0.0f);
+    const int X0 = x0 * 256, Y0 = y0 * 256;
+#pragma unroll
+    for (int t = 0; t < 2; ++t)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            int4 e = make_int4(0, 0, -1, 0), k = make_int4(0, 0, 0, 0);
+            if (valid[t] && small) {
+                const int u = order[t][j], v = order[t][j == 2 ? 0 : j + 1];
+                const int dx = vx[v] - vx[u], dy = vy[v] - vy[u];
+                const bool tl = dy > 0 || (dy == 0 && dx < 0);
+                e = make_int4(dx, dy, dx * (Y0 - vy[u]) - dy * (X0 - vx[u]) - (tl ? 0 : 1), 0);
+                int kq[4] = {0, 0, 0, 0};
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    if (q < a.ns) {
+                        int ox, oy;
+                        sample_offset(a.ns, q, &ox, &oy);
+                        kq[q] = dx * oy - dy * ox;
+                    }
+                }
+                k = make_int4(kq[0], kq[1], kq[2], kq[3]);
+            }
+            f->edge[3 * t + j] = e;
+            f->k[3 * t + j] = k;
+        }
+}
+
+// Covering triangles of each sample of pixel (px, py), 8 bits per sample,
+// for a segment too large for 32-bit edge functions (rare: corners 64 or
+// more pixels apart).
+__device__ __noinline__ uint32_t slow_cover(const float2* xy, const uint32_t* segments, uint32_t s, uint32_t w,
+                                            uint32_t h, int ns, int px, int py) {
+    RenderArgs a{};
+    a.xy = xy;
+    a.segments = segments;
+    a.w = w;
+    a.h = h;
+    SegSetup g;
+    seg_setup(a, s, &g);
+    uint32_t out = 0;
+    for (int q = 0; q < ns; ++q) {
+        int ox, oy;
+        sample_offset(ns, q, &ox, &oy);
+        const long long sx = static_cast<long long>(px) * 256 + ox, sy = static_cast<long long>(py) * 256 + oy;
+        uint32_t n = 0;
+        for (int t = 0; t < 2; ++t)
+            if (g.valid & (1u << t)) n += inside(g.t[t], sx, sy);
+        out |= n << (8 * q);
+    }
+    return out;
 }
 
 // One CTA per tile of T x T pixels (T = 16, 32 or 64). Warp w owns the band
 // of T / 8 rows starting at row w * T / 8; its lanes own the band's pixels
 // (T = 16: lane -> column lane % 16, row lane / 16; T >= 32: columns
 // lane + 32 c, every row of the band) and keep their samples in registers.
-// The CTA sets up 256 segments of the tile's list at a time; each warp
+// The CTA sets up kChunk segments of the tile's list at a time; each warp
 // walks, in draw order, those whose box meets its band (a ballot per 32).
 template <int T>
-__global__ void __launch_bounds__(256) raster_kernel(RenderArgs a) {
+__global__ void __launch_bounds__(256, T == 16 ? 4 : 1) raster_kernel(RenderArgs a) {
     constexpr int kRows = T / 8;
     constexpr int kCols = T >= 32 ? T / 32 : 1;
     constexpr int PPT = T >= 32 ? kRows * kCols : 1;
     constexpr bool kCacheColour = PPT <= 4;
-    __shared__ SegSetup segs[kChunk];
+    __shared__ FastSeg segs[kChunk];
     __shared__ float pal[16][3];
     __shared__ float unorm[256];
     if (threadIdx.x < 48) pal[threadIdx.x / 3][threadIdx.x % 3] = kPalette[a.palette][threadIdx.x / 3][threadIdx.x % 3];
@@ -428,44 +516,52 @@ __global__ void __launch_bounds__(256) raster_kernel(RenderArgs a) {
     for (size_t chunk = begin; chunk < end; chunk += kChunk) {
         const int n = static_cast<int>(min(static_cast<size_t>(kChunk), end - chunk));
         __syncthreads();
-        if (static_cast<int>(threadIdx.x) < n) {
-            SegSetup& g = segs[threadIdx.x];
-            seg_setup(a, a.sorted[chunk + threadIdx.x], &g);
-            if (a.color_by_edge) {
-                palette_color(pal, edge_value(a, g.first), g.col);
-#pragma unroll
-                for (int ch = 0; ch < 3; ++ch) g.col[ch] = __fmul_rn(g.col[ch], 0.1f);
-            }
-        }
+        if (static_cast<int>(threadIdx.x) < n) fast_setup(a, a.sorted[chunk + threadIdx.x], pal, &segs[threadIdx.x]);
         __syncthreads();
         for (int base = 0; base < n; base += 32) {
             const int e0 = base + lane;
-            const bool hit = e0 < n && segs[e0].y0 <= band1 && segs[e0].y1 >= band0;
+            const bool hit = e0 < n && segs[e0].box.y <= band1 && segs[e0].box.w >= band0;
             unsigned mask = __ballot_sync(0xFFFFFFFFu, hit);
             while (mask) {
                 const int e = base + __ffs(mask) - 1;
                 mask &= mask - 1;
-                const SegSetup& g = segs[e];
+                const FastSeg& g = segs[e];
+                const int4 box = g.box;
 #pragma unroll
                 for (int k = 0; k < PPT; ++k) {
-                    if (px[k] < g.x0 || px[k] > g.x1 || py[k] < g.y0 || py[k] > g.y1) continue;
-                    int cover[4];
-                    bool any = false;
+                    if (px[k] < box.x || px[k] > box.z || py[k] < box.y || py[k] > box.w) continue;
+                    int cover[4] = {0, 0, 0, 0};
+                    if (g.flags & kSlow) {
+                        const uint32_t c = slow_cover(a.xy, a.segments, g.seg, a.w, a.h, a.ns, px[k], py[k]);
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        cover[q] = 0;
-                        if (q < a.ns) {
-                            int ox, oy;
-                            sample_offset(a.ns, q, &ox, &oy);
-                            cover[q] = covering(g, px[k] * 256 + ox, py[k] * 256 + oy);
-                            any |= cover[q] != 0;
+                        for (int q = 0; q < 4; ++q) cover[q] = (c >> (8 * q)) & 0xFFu;
+                    } else {
+                        const int rx = (px[k] - box.x) * 256, ry = (py[k] - box.y) * 256;
+                        int p[6];
+#pragma unroll
+                        for (int j = 0; j < 6; ++j) {
+                            const int4 ed = g.edge[j];
+                            p[j] = ed.z + ed.x * ry - ed.y * rx;
+                        }
+                        int4 kk[6];
+#pragma unroll
+                        for (int j = 0; j < 6; ++j) kk[j] = g.k[j];
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            if (q < a.ns) {
+                                auto kq = [&](int j) { return q == 0 ? kk[j].x : q == 1 ? kk[j].y : q == 2 ? kk[j].z : kk[j].w; };
+                                const int t0 = (p[0] + kq(0)) | (p[1] + kq(1)) | (p[2] + kq(2));
+                                const int t1 = (p[3] + kq(3)) | (p[4] + kq(4)) | (p[5] + kq(5));
+                                cover[q] = (t0 >= 0) + (t1 >= 0);
+                            }
                         }
                     }
-                    if (!any) continue;
+                    if ((cover[0] | cover[1] | cover[2] | cover[3]) == 0) continue;
                     float src[3];
                     if (a.color_by_edge) {
-#pragma unroll
-                        for (int ch = 0; ch < 3; ++ch) src[ch] = g.col[ch];
+                        src[0] = g.src.x;
+                        src[1] = g.src.y;
+                        src[2] = g.src.z;
                     } else if (kCacheColour) {
 #pragma unroll
                         for (int ch = 0; ch < 3; ++ch) src[ch] = pcol[kCacheColour ? k : 0][ch];
@@ -474,10 +570,17 @@ __global__ void __launch_bounds__(256) raster_kernel(RenderArgs a) {
 #pragma unroll
                         for (int ch = 0; ch < 3; ++ch) src[ch] = __fmul_rn(src[ch], 0.1f);
                     }
+                    // Samples with the same history blend to the same value.
+                    uint32_t last_in = 0xFFFFFFFFu, last_out = 0;
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
-                        if (cover[q] > 0) samp[k][q] = blend(samp[k][q], src, unorm);
-                        if (cover[q] > 1) samp[k][q] = blend(samp[k][q], src, unorm);
+                        for (int r = 0; r < cover[q]; ++r) {
+                            if (samp[k][q] != last_in) {
+                                last_in = samp[k][q];
+                                last_out = blend(last_in, src, unorm);
+                            }
+                            samp[k][q] = last_out;
+                        }
                     }
                 }
             }
