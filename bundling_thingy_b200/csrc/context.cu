@@ -1194,6 +1194,10 @@ bt_status bt_render(bt_ctx* c, uint8_t* rgba, size_t rgba_bytes, uint64_t* color
         if (device_ms) BT_CUDA(c, cudaEventRecord(c->t0, c->stream));
         if (bt_status s = render_frame(c, xy, device_ms != nullptr, rgba, &colored, &pairs)) return s;
         if (pairs > c->render_cap) return fail(c, BT_ERR_CUDA, "render bin count changed between passes");
+    } else if (pairs + pairs / 2 < c->render_cap) {
+        // Fewer bins than provided for: size the next frame's histogram for
+        // this one's (the buffers keep their size).
+        c->render_cap = pairs + pairs / 4 + 4096;
     }
     if (device_ms) BT_CUDA(c, cudaEventElapsedTime(device_ms, c->t0, c->t1));
     if (colored_pixels) *colored_pixels = colored;

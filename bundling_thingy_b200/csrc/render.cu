@@ -323,7 +323,9 @@ __global__ void __launch_bounds__(256) bin_hist_kernel(RenderArgs a) {
 }
 
 // Stable scatter: the block's pairs in order, each placed after the earlier
-// pairs of its tile (ranks from a warp-wide match on the tile).
+// pairs of its tile (ranks from a warp-wide match on the tile). One warp
+// walks the block 32 pairs at a time, with the loads of the next four
+// batches in flight.
 __global__ void __launch_bounds__(256) bin_rank_kernel(RenderArgs a) {
     extern __shared__ uint32_t next[];
     const uint32_t tiles = a.tiles_x * a.tiles_y;
@@ -331,19 +333,28 @@ __global__ void __launch_bounds__(256) bin_rank_kernel(RenderArgs a) {
         next[t] = a.hist_off[static_cast<size_t>(t) * gridDim.x + blockIdx.x];
     __syncthreads();
     if (threadIdx.x >= 32) return;
+    constexpr int kAhead = 4;
     const int lane = threadIdx.x;
     const unsigned lower = (1u << lane) - 1u;
     const size_t begin = static_cast<size_t>(blockIdx.x) * kBinItems;
     const size_t end = min(begin + kBinItems, live_pairs(a));
-    for (size_t base = begin; base < end; base += 32) {
-        const size_t i = base + lane;
-        const bool valid = i < end;
-        const uint32_t tile = valid ? a.pair_tile[i] : 0xFFFFFFFFu;
-        const unsigned peers = __match_any_sync(0xFFFFFFFFu, tile);
-        if (valid) a.sorted[next[tile] + __popc(peers & lower)] = a.pair_seg[i];
-        __syncwarp();
-        if (valid && lane == 31 - __clz(peers)) next[tile] += __popc(peers);
-        __syncwarp();
+    for (size_t base = begin; base < end; base += 32 * kAhead) {
+        uint32_t tile[kAhead], seg[kAhead];
+#pragma unroll
+        for (int u = 0; u < kAhead; ++u) {
+            const size_t i = base + 32 * u + lane;
+            tile[u] = i < end ? a.pair_tile[i] : 0xFFFFFFFFu;
+            seg[u] = i < end ? a.pair_seg[i] : 0u;
+        }
+#pragma unroll
+        for (int u = 0; u < kAhead; ++u) {
+            const bool valid = tile[u] != 0xFFFFFFFFu;
+            const unsigned peers = __match_any_sync(0xFFFFFFFFu, tile[u]);
+            if (valid) a.sorted[next[tile[u]] + __popc(peers & lower)] = seg[u];
+            __syncwarp();
+            if (valid && lane == 31 - __clz(peers)) next[tile[u]] += __popc(peers);
+            __syncwarp();
+        }
     }
 }
 
@@ -465,7 +476,7 @@ __device__ __noinline__ uint32_t slow_cover(const float2* xy, const uint32_t* se
 // The CTA sets up kChunk segments of the tile's list at a time; each warp
 // walks, in draw order, those whose box meets its band (a ballot per 32).
 template <int T>
-__global__ void __launch_bounds__(256, T == 16 ? 4 : 1) raster_kernel(RenderArgs a) {
+__global__ void __launch_bounds__(256, T == 16 ? 6 : 1) raster_kernel(RenderArgs a) {
     constexpr int kRows = T / 8;
     constexpr int kCols = T >= 32 ? T / 32 : 1;
     constexpr int PPT = T >= 32 ? kRows * kCols : 1;
