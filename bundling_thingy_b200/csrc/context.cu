@@ -39,6 +39,58 @@ bt_status fail(bt_ctx* c, bt_status code, const std::string& msg) {
     return code;
 }
 
+// Bounds of the control points (graph.rs:39-40, 79-91) with the result of
+// a sequential std::min / std::max fold (the earlier value stays on ties);
+// false when a coordinate is not finite. Sixteen interleaved lanes (even: x,
+// odd: y) let the compiler vectorise the pass; a bound that comes out as a
+// zero is refolded in order, since lanes could pick the other zero sign.
+bool point_bounds(const float* xy, uint32_t n, float mn[2], float mx[2]) {
+    constexpr int kLanes = 16;
+    float lo[kLanes], hi[kLanes];
+    uint32_t bad[kLanes];
+    for (int j = 0; j < kLanes; ++j) {
+        lo[j] = 3.40282347e+38f;
+        hi[j] = -3.40282347e+38f;
+        bad[j] = 0;
+    }
+    const size_t m = 2ull * n, body = m / kLanes * kLanes;
+    for (size_t k = 0; k < body; k += kLanes)
+        for (int j = 0; j < kLanes; ++j) {
+            const float v = xy[k + j];
+            uint32_t b;
+            std::memcpy(&b, &v, 4);
+            bad[j] |= static_cast<uint32_t>((b & 0x7F800000u) == 0x7F800000u);
+            lo[j] = v < lo[j] ? v : lo[j];
+            hi[j] = hi[j] < v ? v : hi[j];
+        }
+    uint32_t nonfinite = 0;
+    for (int j = 0; j < kLanes; ++j) nonfinite |= bad[j];
+    for (size_t k = body; k < m; ++k) nonfinite |= static_cast<uint32_t>(!std::isfinite(xy[k]));
+    if (nonfinite) return false;
+    for (int d = 0; d < 2; ++d) {
+        float a = 3.40282347e+38f, b = -3.40282347e+38f;
+        for (int j = d; j < kLanes; j += 2) {
+            a = lo[j] < a ? lo[j] : a;
+            b = b < hi[j] ? hi[j] : b;
+        }
+        for (size_t k = body + d; k < m; k += 2) {
+            a = xy[k] < a ? xy[k] : a;
+            b = b < xy[k] ? xy[k] : b;
+        }
+        if (a == 0.0f || b == 0.0f) {
+            a = 3.40282347e+38f;
+            b = -3.40282347e+38f;
+            for (size_t k = d; k < m; k += 2) {
+                a = xy[k] < a ? xy[k] : a;
+                b = b < xy[k] ? xy[k] : b;
+            }
+        }
+        mn[d] = a;
+        mx[d] = b;
+    }
+    return true;
+}
+
 bt_status cuda_fail(bt_ctx* c, cudaError_t e, const char* what) {
     const bt_status code = (e == cudaErrorMemoryAllocation) ? BT_ERR_BUDGET : BT_ERR_CUDA;
     return fail(c, code, std::string(what) + ": " + cudaGetErrorString(e));
@@ -553,15 +605,8 @@ bt_status bt::upload_begin(bt_ctx* c, const float* xy, uint32_t n_points, const 
     for (uint32_t e = 0; e + 1 < n_starts; ++e)
         if (starts[e + 1] < starts[e] || starts[e + 1] - starts[e] < 2)
             return fail(c, BT_ERR_INVALID, "every edge needs at least two control points");
-    float mn[2] = {3.40282347e+38f, 3.40282347e+38f}, mx[2] = {-3.40282347e+38f, -3.40282347e+38f};
-    for (uint32_t i = 0; i < n_points; ++i) {
-        const float x = xy[2 * i], y = xy[2 * i + 1];
-        if (!std::isfinite(x) || !std::isfinite(y)) return fail(c, BT_ERR_INVALID, "non-finite TRL coordinate");
-        mn[0] = std::fmin(mn[0], x);
-        mn[1] = std::fmin(mn[1], y);
-        mx[0] = std::fmax(mx[0], x);
-        mx[1] = std::fmax(mx[1], y);
-    }
+    float mn[2], mx[2];
+    if (!point_bounds(xy, n_points, mn, mx)) return fail(c, BT_ERR_INVALID, "non-finite TRL coordinate");
     float nm[5];
     std::string err;
     if (!bt::normalization(mn, mx, nm, &err)) return fail(c, BT_ERR_INVALID, err);
