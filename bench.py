@@ -348,8 +348,11 @@ def run_ours(args, ranks: Ranks):
     if ranks.rank == 0 and ranks.world == 1 and not args.no_cpu_baseline:
         cpu = cpu_sample(w, target_seconds=args.cpu_seconds)
 
-    # mean, cell table, scatter, slot prefix (single-pass scans), blur H + V, normalise
-    per_iter = 7
+    # Per iteration (profiles/launches_large.md): neighbour mean, cell table
+    # (tile-sum scan + apply), scatter, slot prefix (reduce + tile-sum scan +
+    # apply) on the context's stream; blur H, blur V + maximum, normalise
+    # (+ a tail launch when the map is not a multiple of 4 texels) beside them.
+    per_iter = 10
     if (w.width * w.height) % 4:
         per_iter += 1
     line = {
