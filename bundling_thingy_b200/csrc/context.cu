@@ -597,7 +597,9 @@ bt_status bt::upload_begin(bt_ctx* c, const float* xy, uint32_t n_points, const 
     c->samples = 0;
     c->iterations = 0;
     c->density_passes = 0;
-    drop_graphs(c);
+    // The iteration graphs are refreshed at the next iteration (an update of
+    // the executable graph when the new capture has the same shape).
+    c->graph_stale[0] = c->graph_stale[1] = true;
     c->stage_used = 0;
     // Input contract of Graph (graph.rs:7-12, 60-77).
     if (n_starts < 2 || starts[0] != 0 || starts[n_starts - 1] != n_points)
@@ -837,7 +839,7 @@ bt_status bt_iterate_async(bt_ctx* c, uint32_t n) {
         const uint32_t pass = c->density_passes;
         if (use_graphs) {
             cudaGraphExec_t& exec = c->graphs[c->cur];
-            if (!exec) {
+            if (!exec || c->graph_stale[c->cur]) {
                 cudaGraph_t graph = nullptr;
                 BT_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
                 bt_status s = enqueue_iteration(c, c->cur, pass);
@@ -847,12 +849,23 @@ bt_status bt_iterate_async(bt_ctx* c, uint32_t n) {
                     return s;
                 }
                 if (e != cudaSuccess) return cuda_fail(c, e, "cudaStreamEndCapture");
-                e = cudaGraphInstantiate(&exec, graph, 0);
+                if (exec) {
+                    // Same kernels and dependencies as before: update the
+                    // parameters in place; otherwise build it anew.
+                    cudaGraphExecUpdateResultInfo info{};
+                    if (cudaGraphExecUpdate(exec, graph, &info) != cudaSuccess) {
+                        cudaGetLastError();
+                        cudaGraphExecDestroy(exec);
+                        exec = nullptr;
+                    }
+                }
+                if (!exec) e = cudaGraphInstantiate(&exec, graph, 0);
                 cudaGraphDestroy(graph);
                 if (e != cudaSuccess) {
                     exec = nullptr;
                     return cuda_fail(c, e, "cudaGraphInstantiate");
                 }
+                c->graph_stale[c->cur] = false;
             }
             BT_CUDA(c, cudaGraphLaunch(exec, c->stream));
         } else {

@@ -133,6 +133,7 @@ struct bt_ctx {
     int cur = 0;
 
     cudaGraphExec_t graphs[2] = {nullptr, nullptr};
+    bool graph_stale[2] = {false, false};   // a new upload changed sizes or buffers
 
     std::vector<bt::StageRec> stage_pool;
     size_t stage_used = 0;
