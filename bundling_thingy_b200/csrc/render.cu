@@ -93,15 +93,9 @@ struct TriSetup {
 struct SegSetup {
     TriSetup t[2];
     int x0, y0, x1, y1;
-    float col[3];     // palette colour (edge-id colouring; set by the raster kernel)
     uint32_t first;
-    uint32_t valid;   // bit k: triangle k has nonzero area; kSmall: 32-bit edge functions suffice
+    uint32_t valid;   // bit k: triangle k has nonzero area
 };
-
-// Set when the snapped corners span less than 64 pixels in x and in y: every
-// edge function over the segment's pixel box then stays below 2^30 in
-// magnitude and is evaluated exactly in 32 bits.
-constexpr uint32_t kSmall = 4u;
 
 __device__ __forceinline__ long long edge_fn(int ax, int ay, int dx, int dy, long long px, long long py) {
     return static_cast<long long>(dx) * (py - ay) - static_cast<long long>(dy) * (px - ax);
@@ -199,7 +193,6 @@ __device__ __forceinline__ void seg_setup(const RenderArgs& a, uint32_t s, SegSe
         }
     }
     if (!g->valid) return;
-    if (maxx - minx < (1 << 14) && maxy - miny < (1 << 14)) g->valid |= kSmall;
     g->x0 = max(0, minx >> 8);
     g->x1 = min(static_cast<int>(a.w) - 1, maxx >> 8);
     g->y0 = max(0, miny >> 8);
@@ -363,8 +356,9 @@ __global__ void __launch_bounds__(256) bin_rank_kernel(RenderArgs a) {
 constexpr int kChunk = 128;
 constexpr uint32_t kSlow = 1u;
 
-// A segment as the raster kernel tests it. For a small segment (kSmall) the
-// six edge functions of its two triangles are kept relative to the origin
+// A segment as the raster kernel tests it. For a small segment (snapped
+// corners less than 64 pixels apart in x and in y, so every edge function
+// over its pixel box stays below 2^30 in magnitude) the six edge functions of its two triangles are kept relative to the origin
 // (X0, Y0) = 256 * (x0, y0) of its pixel box, with the top-left rule folded
 // in: for edge j, f_j(sx, sy) - bias_j = E_j + dx_j * (sy - Y0) - dy_j * (sx - X0),
 // bias_j = 0 on a top-left edge and 1 otherwise, so a sample is inside
