@@ -66,7 +66,7 @@ class _Options(ctypes.Structure):
         ("fine_cells", ctypes.c_uint32), ("use_graphs", ctypes.c_uint32), ("timing", ctypes.c_uint32),
         ("record_neighbors", ctypes.c_uint32), ("search_mode", ctypes.c_uint32), ("fine_cells_x", ctypes.c_uint32),
         ("palette", ctypes.c_uint32), ("msaa", ctypes.c_uint32), ("endpoint_dots", ctypes.c_uint32),
-        ("reserved", ctypes.c_uint32 * 2),
+        ("advect_step", ctypes.c_float), ("advect_smooth", ctypes.c_float),
     ]
 
 
@@ -243,6 +243,8 @@ class Options:
     palette: int = 0         # PALETTES index (src/palette.rs:13-23): viridis, the reference default
     msaa: int = 4            # samples per pixel: 2 or 4 as the reference (1 accepted)
     endpoint_dots: bool = False
+    advect_step: float = 0.0     # > 0: density-gradient advection (texels per iteration) instead of the mean
+    advect_smooth: float = 0.0   # its Laplacian relaxation along the path, in [0, 1]
 
     def _struct(self) -> _Options:
         o = _Options()
@@ -265,6 +267,8 @@ class Options:
         o.palette = int(self.palette)
         o.msaa = int(self.msaa)
         o.endpoint_dots = int(bool(self.endpoint_dots))
+        o.advect_step = float(self.advect_step)
+        o.advect_smooth = float(self.advect_smooth)
         return o
 
     def resample_scale(self) -> tuple[float, float]:

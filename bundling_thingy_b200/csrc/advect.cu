@@ -1,0 +1,79 @@
+// advect.cu — density-gradient advection, an iteration mode beyond the
+// reference (kernel-density-estimation edge bundling): every sample that is
+// not the first or last of its path climbs the gradient of the blurred,
+// normalised density by a fixed step, then relaxes towards its advected path
+// neighbours; the new positions are splatted for the next density pass. The
+// oracle (or_advect) states the same operation order:
+//  - map position (u, v) = ((x * 0.5 + 0.5) * (W - 1), (0.5 - y * 0.5) * (H - 1))
+//    (the splat's texel space);
+//  - bilinear density with clamp-to-edge; central differences one texel
+//    apart, halved;
+//  - `step` texels along the unit gradient (none when its length is not above
+//    1e-12), back to clip units by 2 / (W - 1) and -2 / (H - 1);
+//  - a + smooth * ((a_prev + a_next) * 0.5 - a).
+// One thread per sample, sample order (paths are contiguous; edge ids change
+// at path boundaries). Every quantity rounds once per operation.
+#include "kernels.cuh"
+
+namespace bt {
+namespace {
+
+__device__ __forceinline__ float density_at(const float* __restrict__ d, uint32_t w, uint32_t h, float u, float v) {
+    const float uc = fminf(fmaxf(u, 0.0f), static_cast<float>(w - 1u));
+    const float vc = fminf(fmaxf(v, 0.0f), static_cast<float>(h - 1u));
+    const float fx0 = floorf(uc), fy0 = floorf(vc);
+    const float fx = __fsub_rn(uc, fx0), fy = __fsub_rn(vc, fy0);
+    const uint32_t x0 = static_cast<uint32_t>(fx0), y0 = static_cast<uint32_t>(fy0);
+    const uint32_t x1 = min(x0 + 1u, w - 1u), y1 = min(y0 + 1u, h - 1u);
+    const float* r0 = d + static_cast<size_t>(y0) * w;
+    const float* r1 = d + static_cast<size_t>(y1) * w;
+    const float top = __fadd_rn(__fmul_rn(__ldg(r0 + x0), __fsub_rn(1.0f, fx)), __fmul_rn(__ldg(r0 + x1), fx));
+    const float bottom = __fadd_rn(__fmul_rn(__ldg(r1 + x0), __fsub_rn(1.0f, fx)), __fmul_rn(__ldg(r1 + x1), fx));
+    return __fadd_rn(__fmul_rn(top, __fsub_rn(1.0f, fy)), __fmul_rn(bottom, fy));
+}
+
+__device__ __forceinline__ float2 advected(const AdvectArgs& a, float2 p) {
+    const float u = __fmul_rn(__fadd_rn(__fmul_rn(p.x, 0.5f), 0.5f), static_cast<float>(a.map.w - 1u));
+    const float v = __fmul_rn(__fsub_rn(0.5f, __fmul_rn(p.y, 0.5f)), static_cast<float>(a.map.h - 1u));
+    const float gu = __fmul_rn(__fsub_rn(density_at(a.density, a.map.w, a.map.h, __fadd_rn(u, 1.0f), v),
+                                         density_at(a.density, a.map.w, a.map.h, __fsub_rn(u, 1.0f), v)),
+                               0.5f);
+    const float gv = __fmul_rn(__fsub_rn(density_at(a.density, a.map.w, a.map.h, u, __fadd_rn(v, 1.0f)),
+                                         density_at(a.density, a.map.w, a.map.h, u, __fsub_rn(v, 1.0f))),
+                               0.5f);
+    const float len = __fsqrt_rn(__fadd_rn(__fmul_rn(gu, gu), __fmul_rn(gv, gv)));
+    float du = 0.0f, dv = 0.0f;
+    if (len > 1e-12f) {
+        du = __fmul_rn(a.step, __fdiv_rn(gu, len));
+        dv = __fmul_rn(a.step, __fdiv_rn(gv, len));
+    }
+    return make_float2(__fadd_rn(p.x, __fmul_rn(du, a.sx_inv)), __fsub_rn(p.y, __fmul_rn(dv, a.sy_inv)));
+}
+
+__device__ __forceinline__ bool movable(const uint32_t* __restrict__ ids, uint32_t n, uint32_t i) {
+    return i > 0 && i + 1 < n && ids[i - 1] == ids[i] && ids[i + 1] == ids[i];
+}
+
+__global__ void __launch_bounds__(256) advect_kernel(AdvectArgs a) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    float2 out = a.xy[i];
+    if (movable(a.edge_ids, a.n, i)) {
+        const float2 s = advected(a, out);
+        const float2 p = movable(a.edge_ids, a.n, i - 1) ? advected(a, a.xy[i - 1]) : a.xy[i - 1];
+        const float2 q = movable(a.edge_ids, a.n, i + 1) ? advected(a, a.xy[i + 1]) : a.xy[i + 1];
+        out.x = __fadd_rn(s.x, __fmul_rn(a.smooth, __fsub_rn(__fmul_rn(__fadd_rn(p.x, q.x), 0.5f), s.x)));
+        out.y = __fadd_rn(s.y, __fmul_rn(a.smooth, __fsub_rn(__fmul_rn(__fadd_rn(p.y, q.y), 0.5f), s.y)));
+    }
+    a.out[i] = out;
+    uint32_t d;
+    if (a.counts && splat_index(out.x, out.y, a.map, &d)) atomicAdd(&a.counts[d], 1u);
+}
+
+}  // namespace
+
+void launch_advect(const AdvectArgs& a, cudaStream_t s) {
+    if (a.n) advect_kernel<<<div_up(a.n, 256), 256, 0, s>>>(a);
+}
+
+}  // namespace bt

@@ -353,6 +353,32 @@ bt_status enqueue_iteration(bt_ctx* c, int src, uint32_t pass) {
     return s;
 }
 
+// One density-gradient advection step (advect.cu) from the current
+// positions (sample order, tmp_xy) into adv_xy, fused with their splat, then
+// density pass `pass` of the new positions; the buffers swap afterwards.
+bt_status enqueue_advection(bt_ctx* c, uint32_t pass) {
+    BT_CUDA(c, cudaMemsetAsync(c->counts.p, 0, c->texels * sizeof(uint32_t), c->stream));
+    BT_CUDA(c, cudaMemsetAsync(c->peak.p, 0, sizeof(uint32_t), c->stream));
+    stage_begin(c, "graph.advect");
+    bt::AdvectArgs a{};
+    a.xy = c->tmp_xy.as<float2>();
+    a.edge_ids = c->edge_ids.as<uint32_t>();
+    a.n = c->samples;
+    a.density = c->norm.as<float>();
+    a.map = c->map;
+    a.step = c->opt.advect_step;
+    a.smooth = c->opt.advect_smooth;
+    a.sx_inv = 2.0f / static_cast<float>(c->map.w - 1u);
+    a.sy_inv = 2.0f / static_cast<float>(c->map.h - 1u);
+    a.out = c->adv_xy.as<float2>();
+    a.counts = c->counts.as<uint32_t>();
+    bt::launch_advect(a, c->stream);
+    stage_end(c);
+    if (bt_status s = enqueue_density(c, pass, c->stream)) return s;
+    std::swap(c->tmp_xy, c->adv_xy);
+    return BT_OK;
+}
+
 bt_status validate_options(const bt_options* o, bt_ctx* c) {
     if (o->width == 0 || o->height == 0) return fail(c, BT_ERR_INVALID, "density map dimensions must be nonzero");
     if (o->width > kMaxDimension || o->height > kMaxDimension)
@@ -372,6 +398,13 @@ bt_status validate_options(const bt_options* o, bt_ctx* c) {
         return fail(c, BT_ERR_INVALID, "fine_cells too large");
     if (o->search_mode > 1) return fail(c, BT_ERR_INVALID, "unknown search_mode");
     if (o->palette > BT_PALETTE_BATLOW) return fail(c, BT_ERR_INVALID, "unknown palette");
+    if (!(o->advect_step >= 0.0f) || !std::isfinite(o->advect_step) || !(o->advect_smooth >= 0.0f) ||
+        !(o->advect_smooth <= 1.0f))
+        return fail(c, BT_ERR_INVALID, "advection step must be finite and >= 0, smoothing in [0, 1]");
+    if (o->advect_step > 0.0f && o->neighbor_radius > 0)
+        return fail(c, BT_ERR_INVALID, "choose one bundling step: the neighbour mean or density advection");
+    if (o->advect_step > 0.0f && (o->width < 2 || o->height < 2))
+        return fail(c, BT_ERR_INVALID, "density advection needs a map of at least 2 x 2 texels");
     if (o->msaa != 0 && o->msaa != 1 && o->msaa != 2 && o->msaa != 4)
         return fail(c, BT_ERR_INVALID, "msaa must be 1, 2 or 4 samples");
     const uint64_t grid = o->neighbor_radius ? reference_grid_bytes(o->width, o->height, o->neighbor_radius) : 0;
@@ -473,7 +506,7 @@ void bt_destroy(bt_ctx* c) {
                       &c->cell_start, &c->hist_tiles, &c->counts, &c->himg, &c->vimg, &c->norm, &c->peak,
                       &c->records, &c->integrals, &c->r_seg_count, &c->r_seg_off, &c->r_scan64,
                       &c->r_pair_tile, &c->r_pair_seg, &c->r_sorted, &c->r_hist, &c->r_hist_off, &c->r_scan32,
-                      &c->r_samples, &c->r_rgba, &c->r_misc};
+                      &c->r_samples, &c->r_rgba, &c->r_misc, &c->adv_xy};
     for (DevBuf* b : bufs) release(*b, c->stream);
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->account) c->account->used -= c->device_bytes;
@@ -528,7 +561,7 @@ bt_status bt::create_context(const bt_options* options, bt::MemAccount* account,
     const uint32_t W = options->width, H = options->height;
     c->map = bt::Map{W, H, static_cast<float>(W - 1u), static_cast<float>(H - 1u)};
     c->texels = static_cast<size_t>(W) * H;
-    c->accumulate = options->color_by == BT_COLOR_BY_DENSITY;
+    c->accumulate = options->color_by == BT_COLOR_BY_DENSITY || options->advect_step > 0.0f;
     if (options->sample_spacing > 0.0f) {
         c->rsx = c->rsy = static_cast<float>(0.5 / static_cast<double>(options->sample_spacing));
     } else {
@@ -830,10 +863,22 @@ bt_status bt_upload_graph(bt_ctx* c, const bt_graph* g, uint32_t* out_samples) {
 
 bt_status bt_iterate_async(bt_ctx* c, uint32_t n) {
     if (!c) return fail(nullptr, BT_ERR_INVALID, "null context");
-    if (!c->has_grid) return fail(c, BT_ERR_NOT_CONFIGURED, "neighbor radius is not configured");
+    const bool advect = c->opt.advect_step > 0.0f;
+    if (!c->has_grid && !advect) return fail(c, BT_ERR_NOT_CONFIGURED, "neighbor radius is not configured");
     if (!c->uploaded) return fail(c, BT_ERR_NO_GRAPH, "no uploaded graph");
     cudaSetDevice(c->device);
     c->stage_used = 0;
+    if (advect) {
+        if (bt_status s = ensure(c, c->adv_xy, 8ull * c->samples)) return s;
+        for (uint32_t i = 0; i < n; ++i) {
+            if (bt_status s = enqueue_advection(c, c->density_passes)) return s;
+            c->iterations++;
+            c->density_passes++;
+        }
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return cuda_fail(c, e, "kernel launch");
+        return BT_OK;
+    }
     const bool use_graphs = c->opt.use_graphs && !c->opt.timing && constant_sigma(c->opt);
     for (uint32_t i = 0; i < n; ++i) {
         const uint32_t pass = c->density_passes;

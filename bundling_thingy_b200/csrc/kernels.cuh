@@ -159,6 +159,21 @@ void launch_positions_from_slots(const uint4* rec, const uint32_t* tag, uint32_t
 void launch_edge_integrals(const PathRec* paths, uint32_t n_paths, const float2* original, const float2* current,
                            double* out, uint32_t* status, cudaStream_t s);
 
+// ---- density-gradient advection (advect.cu) ----
+struct AdvectArgs {
+    const float2* xy;            // current positions, sample order
+    const uint32_t* edge_ids;    // per sample (paths are contiguous)
+    uint32_t n;
+    const float* density;        // normalised density of xy, map.w x map.h
+    Map map;
+    float step;                  // texels per iteration
+    float smooth;                // Laplacian relaxation weight
+    float sx_inv, sy_inv;        // 2 / (W - 1), 2 / (H - 1)
+    float2* out;                 // new positions, sample order
+    uint32_t* counts;            // splat of the new positions (zero before)
+};
+void launch_advect(const AdvectArgs& a, cudaStream_t s);
+
 // ---- rendering (render.cu) ----
 // Pairs per block of the stable tile sort; tiles per frame at most (the sort
 // keeps one 4-byte counter per tile in shared memory).

@@ -66,7 +66,6 @@ bt_options normalized_options(const bt_options& in, int32_t device) {
     bt_options o = in;
     o.device = device;
     o.timing = 0;
-    std::memset(o.reserved, 0, sizeof(o.reserved));
     return o;
 }
 

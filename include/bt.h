@@ -73,7 +73,11 @@ typedef struct bt_options {
     uint32_t palette;               /* --palette: BT_PALETTE_* */
     uint32_t msaa;                  /* --msaa: 2 or 4 samples per pixel (1 also accepted); 0 = 4 */
     uint32_t endpoint_dots;         /* --endpoint-dots: dots at the first and last sample of each path */
-    uint32_t reserved[2];
+    /* Density-gradient advection, an iteration mode beyond the reference
+       (kernel-density-estimation bundling; 0 = the neighbour mean): */
+    float advect_step;              /* texels per iteration up the density gradient; > 0 selects the mode
+                                       (neighbor_radius must then be 0; density is always accumulated) */
+    float advect_smooth;            /* Laplacian relaxation towards the path neighbours, in [0, 1] */
 } bt_options;
 
 typedef struct bt_info {
@@ -124,8 +128,9 @@ bt_status bt_upload(bt_ctx* ctx, const float* xy, uint32_t n_points, const uint3
 bt_status bt_upload_graph(bt_ctx* ctx, const bt_graph* graph, uint32_t* out_samples);
 
 /* Gpu::iterate (src/gpu.rs:527-553), n times: neighbour mean fused with the
- * density splat, grid rebuild, blur and normalisation. Returns after the work
- * has finished on the device. */
+ * density splat, grid rebuild, blur and normalisation (or, with advect_step,
+ * one density-gradient advection step fused with the splat, then blur and
+ * normalisation). Returns after the work has finished on the device. */
 bt_status bt_iterate(bt_ctx* ctx, uint32_t n);
 
 /* Enqueue n iterations without waiting (bt_synchronize waits). */

@@ -95,6 +95,8 @@ def lib():
         L.or_neighbor_mean_sample.restype = ctypes.c_size_t
         L.or_squared_integral.argtypes = [_f32p, ctypes.c_size_t, _f32p, ctypes.c_size_t, _f64p]
         L.or_distortion.argtypes = [_u32p, ctypes.c_uint32, _f32p, _f32p, ctypes.c_uint32, _f64p, _f64p]
+        L.or_advect.argtypes = [_f32p, _u32p, ctypes.c_size_t, _f32p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_float,
+                                ctypes.c_float, _f32p]
         L.or_half_round.argtypes = [ctypes.c_float]
         L.or_half_round.restype = ctypes.c_float
         L.or_render.argtypes = [_f32p, _u32p, _u32p, ctypes.c_uint32, ctypes.c_uint32, _f32p, ctypes.c_uint32,
@@ -233,6 +235,17 @@ def distortion(paths, original_xy, current_xy, size):
     if rc:
         raise OracleError(rc, "distortion failed")
     return d.value, r.value
+
+
+def advect(xy, edge_ids, density, w, h, step, smooth):
+    """One density-gradient advection step (oracle.cpp or_advect)."""
+    xy = np.ascontiguousarray(xy, np.float32).reshape(-1, 2)
+    edge_ids = np.ascontiguousarray(edge_ids, np.uint32)
+    density = np.ascontiguousarray(density, np.float32).reshape(-1)
+    out = np.empty_like(xy)
+    lib().or_advect(_p(xy, _f32p), _p(edge_ids, _u32p), xy.shape[0], _p(density, _f32p), w, h, np.float32(step),
+                    np.float32(smooth), _p(out, _f32p))
+    return out
 
 
 def half_round(v: float) -> float:

@@ -909,3 +909,81 @@ extern "C" int or_distortion(const uint32_t* paths, uint32_t n_paths, const floa
     if (!std::isfinite(*distortion) || !std::isfinite(*rms_pixels)) return 3;
     return 0;
 }
+
+// ---------------------------------------------------------------------------
+// Density-gradient advection step (an extension beyond the reference, in the
+// manner of kernel-density-estimation edge bundling: samples climb the
+// gradient of the blurred density, then relax along their path). The CUDA
+// kernel (csrc/advect.cu) follows the same operation order:
+//  - map position (u, v) = ((x * 0.5 + 0.5) * (W - 1), (0.5 - y * 0.5) * (H - 1)),
+//    the splat's texel space;
+//  - density sampled bilinearly with clamp-to-edge; gradient by central
+//    differences one texel apart, halved;
+//  - a step of `step` texels along the unit gradient (none when its length is
+//    not above 1e-12), back to clip units by 2 / (W - 1) and -2 / (H - 1);
+//  - Laplacian relaxation a + smooth * ((a_prev + a_next) * 0.5 - a) with the
+//    advected neighbours along the path; first and last samples stay fixed.
+namespace {
+
+float density_at(const float* d, uint32_t w, uint32_t h, float u, float v) {
+    const float uc = std::fmin(std::fmax(u, 0.0f), static_cast<float>(w - 1u));
+    const float vc = std::fmin(std::fmax(v, 0.0f), static_cast<float>(h - 1u));
+    const float fx0 = std::floor(uc), fy0 = std::floor(vc);
+    const float fx = uc - fx0, fy = vc - fy0;
+    const uint32_t x0 = static_cast<uint32_t>(fx0), y0 = static_cast<uint32_t>(fy0);
+    const uint32_t x1 = std::min(x0 + 1u, w - 1u), y1 = std::min(y0 + 1u, h - 1u);
+    const float top = d[static_cast<size_t>(y0) * w + x0] * (1.0f - fx) + d[static_cast<size_t>(y0) * w + x1] * fx;
+    const float bottom = d[static_cast<size_t>(y1) * w + x0] * (1.0f - fx) + d[static_cast<size_t>(y1) * w + x1] * fx;
+    return top * (1.0f - fy) + bottom * fy;
+}
+
+void advected(const float* xy, size_t i, const float* d, uint32_t w, uint32_t h, float step, float sxi, float syi,
+              float* out) {
+    const float x = xy[2 * i], y = xy[2 * i + 1];
+    const float u = (x * 0.5f + 0.5f) * static_cast<float>(w - 1u);
+    const float v = (0.5f - y * 0.5f) * static_cast<float>(h - 1u);
+    const float gu = (density_at(d, w, h, u + 1.0f, v) - density_at(d, w, h, u - 1.0f, v)) * 0.5f;
+    const float gv = (density_at(d, w, h, u, v + 1.0f) - density_at(d, w, h, u, v - 1.0f)) * 0.5f;
+    const float len = std::sqrt(gu * gu + gv * gv);
+    float du = 0.0f, dv = 0.0f;
+    if (len > 1e-12f) {
+        du = step * (gu / len);
+        dv = step * (gv / len);
+    }
+    out[0] = x + du * sxi;
+    out[1] = y - dv * syi;
+}
+
+}  // namespace
+
+extern "C" void or_advect(const float* xy, const uint32_t* edge_ids, size_t n, const float* density, uint32_t w,
+                          uint32_t h, float step, float smooth, float* out_xy) {
+    const float sxi = 2.0f / static_cast<float>(w - 1u), syi = 2.0f / static_cast<float>(h - 1u);
+    auto movable = [&](size_t i) {
+        return i > 0 && i + 1 < n && edge_ids[i - 1] == edge_ids[i] && edge_ids[i + 1] == edge_ids[i];
+    };
+#pragma omp parallel for schedule(static)
+    for (long long ii = 0; ii < static_cast<long long>(n); ++ii) {
+        const size_t i = static_cast<size_t>(ii);
+        if (!movable(i)) {
+            out_xy[2 * i] = xy[2 * i];
+            out_xy[2 * i + 1] = xy[2 * i + 1];
+            continue;
+        }
+        float a[2], p[2], q[2];
+        advected(xy, i, density, w, h, step, sxi, syi, a);
+        if (movable(i - 1)) {
+            advected(xy, i - 1, density, w, h, step, sxi, syi, p);
+        } else {
+            p[0] = xy[2 * (i - 1)];
+            p[1] = xy[2 * (i - 1) + 1];
+        }
+        if (movable(i + 1)) {
+            advected(xy, i + 1, density, w, h, step, sxi, syi, q);
+        } else {
+            q[0] = xy[2 * (i + 1)];
+            q[1] = xy[2 * (i + 1) + 1];
+        }
+        for (int k = 0; k < 2; ++k) out_xy[2 * i + k] = a[k] + smooth * ((p[k] + q[k]) * 0.5f - a[k]);
+    }
+}

@@ -104,6 +104,14 @@ int or_squared_integral(const float* original, size_t n_original, const float* c
 int or_distortion(const uint32_t* paths, uint32_t n_paths, const float* original_xy,
                   const float* current_xy, uint32_t size, double* distortion, double* rms_pixels);
 
+/* One density-gradient advection step (an extension beyond the reference):
+ * every sample that is not the first or last of its path (edge_ids differ at
+ * path boundaries) moves `step` texels up the gradient of `density` (w*h,
+ * the normalised map), then relaxes towards the mean of its advected path
+ * neighbours by `smooth`. */
+void or_advect(const float* xy, const uint32_t* edge_ids, size_t n, const float* density, uint32_t w, uint32_t h,
+               float step, float smooth, float* out_xy);
+
 /* Path rasterisation and the noisiness count (render.cpp): RGBA8 of w*h
  * pixels and the number of pixels whose RGB differs from the background.
  * palette 0 viridis, 1 cividis, 2 plasma, 3 batlow; msaa 1, 2 or 4; paths
