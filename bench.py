@@ -51,7 +51,9 @@ def parse_args():
     p.add_argument("--e2e-jobs", type=int, default=3)
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU work of the baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--workload", choices=["large", "batched", "served", "render"], default="large")
+    p.add_argument("--workload", choices=["large", "batched", "served", "render", "advect"], default="large")
+    p.add_argument("--advect-step", type=float, default=1.0, help="advect workload: texels per iteration")
+    p.add_argument("--advect-smooth", type=float, default=0.5, help="advect workload: path relaxation weight")
     p.add_argument("--render-iterations", type=int, default=30,
                    help="render workload: mean updates before the frames are drawn")
     p.add_argument("--graphs", type=int, default=256, help="batched workload: number of graphs")
@@ -459,6 +461,61 @@ def run_render(args, ranks: Ranks):
         print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------- advect
+def run_advect(args, ranks: Ranks):
+    """Iterations of the density-gradient advection mode (an extension beyond
+    the reference) on the large workload, against the oracle's step with its
+    splat, blur and normalisation on all host threads."""
+    import bundling_thingy_b200 as bt
+
+    w = workload(args.edges)
+    device = ranks.local
+    opts = bt.Options(width=w.width, height=w.height, sample_spacing=w.spacing, blur_sigma=w.sigma, device=device,
+                      advect_step=args.advect_step, advect_smooth=args.advect_smooth)
+    gpu = bt.Gpu(opts)
+    n = gpu.upload((w.xy, w.starts))
+    gpu.iterate(max(args.warmup, 3))
+    sampler = ClockSampler(device)
+    sampler.start()
+    ranks.barrier()
+    ms = gpu.iterate_timed(args.steps)
+    ranks.barrier()
+    clocks = sampler.stop()
+    ms_max = ranks.max(ms)
+    value = ranks.sum(float(n) * args.steps) / (ms_max / 1e3)
+    cpu = None
+    if ranks.rank == 0 and ranks.world == 1 and not args.no_cpu_baseline:
+        import oracle as O
+
+        xy, ids = gpu.read_points()
+        dens = gpu.read_density()
+        taps = O.blur_weights(float(np.float32(w.sigma)))
+        t0 = time.perf_counter()
+        out = O.advect(xy, ids, dens, w.width, w.height, args.advect_step, args.advect_smooth)
+        counts = O.splat(out, w.width, w.height)
+        _, vt, peak = O.blur(counts, w.width, w.height, taps)
+        O.normalize(vt, peak)
+        t_cpu = time.perf_counter() - t0
+        threads = len(os.sched_getaffinity(0))
+        cpu = {"value": n / t_cpu, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"one whole iteration ({n} samples): advection step with OpenMP over {threads} host "
+                         f"threads, splat, blur and normalisation"}
+    gpu.close()
+    line = {
+        "metric": METRIC.replace("at 100k edges", "at 100k edges, advection mode"), "value": value, "unit": UNIT,
+        "n_gpus": ranks.world, "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms_max / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded random-walk polylines)",
+        "config": {"workload": (f"advect: large ({n} samples, 2048^2, sigma {w.sigma}), step "
+                                f"{args.advect_step} texels, smoothing {args.advect_smooth}"),
+                   "l2": "inputs larger than L2"},
+        "clocks": clocks,
+        "cpu_baseline": cpu,
+    }
+    if ranks.rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 # ---------------------------------------------------------------- batched
 def run_batched(args, ranks: Ranks):
     """256 independent graphs (edges log-uniform 200-20,000, grids 256/512/1024),
@@ -773,6 +830,8 @@ def main():
             run_served(args, ranks)
         elif args.workload == "render":
             run_render(args, ranks)
+        elif args.workload == "advect":
+            run_advect(args, ranks)
         else:
             run_ours(args, ranks)
     finally:
