@@ -36,9 +36,9 @@ METRIC = "points·iter/s at 100k edges"
 UNIT = "points·iter/s"
 ITERATIONS_PER_JOB = 30
 # Algorithmic bytes per sample of the fused neighbour-mean kernel: read
-# position 8 + fixed-point position 8 + tag 4; write position 8 + tag 4 +
-# next search cell 4; population atomic 4 + splat atomic 4.
-MEAN_BYTES_PER_SAMPLE = 44
+# position record 8 + tag 4; write position 8 + tag 4 + next search cell 4;
+# population atomic 4 + splat atomic 4.
+MEAN_BYTES_PER_SAMPLE = 36
 
 
 def parse_args():

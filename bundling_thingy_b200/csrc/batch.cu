@@ -53,7 +53,7 @@ struct SlotDesc {
     const uint32_t* hist;
     uint32_t* cell_start;
     uint32_t* cell_sums;     // population sums per cell tile (from the mean), scanned in place (cell_tiles + 1)
-    const uint4* rec[2];     // records by slot parity
+    const float2* rec[2];    // records by slot parity
     LL2* slot_prefix;
     LL2* prefix_sums;        // position sums per prefix tile, scanned in place (prefix_tiles + 1)
     uint32_t cells;
@@ -375,7 +375,7 @@ bt_status fill_taps(bt_batch* b, Slot& s, uint32_t upto) {
 
 MeanArgs mean_args(bt_ctx* c, int src) {
     MeanArgs m{};
-    m.rec = c->sorted_rec[src].as<uint4>();
+    m.rec = c->sorted_rec[src].as<float2>();
     m.tag = c->sorted_tag[src].as<uint32_t>();
     m.cell_start = c->cell_start.as<uint32_t>();
     m.prefix = c->slot_prefix.as<LL2>();
@@ -399,7 +399,7 @@ ScatterArgs scatter_args(bt_ctx* c, int src, uint32_t* status) {
     s.cell = c->tmp_cell.as<uint32_t>();
     s.cell_start = c->cell_start.as<uint32_t>();
     s.hist = c->hist.as<uint32_t>();
-    s.out_rec = c->sorted_rec[src ^ 1].as<uint4>();
+    s.out_rec = c->sorted_rec[src ^ 1].as<float2>();
     s.out_tag = c->sorted_tag[src ^ 1].as<uint32_t>();
     s.n = c->samples;
     s.cells = static_cast<uint32_t>(c->cells);
@@ -462,8 +462,8 @@ bt_status rebuild(bt_batch* b) {
         d.hist = c->hist.as<uint32_t>();
         d.cell_start = c->cell_start.as<uint32_t>();
         d.cell_sums = c->hist_tiles.as<uint32_t>();
-        d.rec[0] = c->sorted_rec[0].as<uint4>();
-        d.rec[1] = c->sorted_rec[1].as<uint4>();
+        d.rec[0] = c->sorted_rec[0].as<float2>();
+        d.rec[1] = c->sorted_rec[1].as<float2>();
         d.slot_prefix = c->slot_prefix.as<LL2>();
         d.prefix_sums = c->prefix_tiles.as<LL2>();
         d.cells = static_cast<uint32_t>(c->cells);

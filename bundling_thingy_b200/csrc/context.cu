@@ -299,7 +299,7 @@ void enqueue_binning(bt_ctx* c, int dst, bool tiles_ready) {
     s.cell = c->tmp_cell.as<uint32_t>();
     s.cell_start = c->cell_start.as<uint32_t>();
     s.hist = c->hist.as<uint32_t>();
-    s.out_rec = c->sorted_rec[dst].as<uint4>();
+    s.out_rec = c->sorted_rec[dst].as<float2>();
     s.out_tag = c->sorted_tag[dst].as<uint32_t>();
     s.n = c->samples;
     s.cells = static_cast<uint32_t>(c->cells);
@@ -307,7 +307,7 @@ void enqueue_binning(bt_ctx* c, int dst, bool tiles_ready) {
     bt::launch_scatter(s, c->stream);
     stage_end(c);
     stage_begin(c, "graph.slot_prefix");
-    bt::launch_slot_prefix(c->sorted_rec[dst].as<uint4>(), c->samples, c->slot_prefix.as<bt::LL2>(),
+    bt::launch_slot_prefix(c->sorted_rec[dst].as<float2>(), c->samples, c->slot_prefix.as<bt::LL2>(),
                            c->prefix_tiles.as<bt::LL2>(), c->stream);
     stage_end(c);
 }
@@ -321,7 +321,7 @@ bt_status enqueue_iteration(bt_ctx* c, int src, uint32_t pass) {
     cudaMemsetAsync(c->hist_tiles.p, 0, c->hist_tiles.bytes, c->stream);
     stage_begin(c, "graph.neighbor_mean");
     bt::MeanArgs m{};
-    m.rec = c->sorted_rec[src].as<uint4>();
+    m.rec = c->sorted_rec[src].as<float2>();
     m.tag = c->sorted_tag[src].as<uint32_t>();
     m.cell_start = c->cell_start.as<uint32_t>();
     m.prefix = c->slot_prefix.as<bt::LL2>();
@@ -718,7 +718,7 @@ bt_status bt::upload_finish(bt_ctx* c) {
     if (bt_status s = ensure(c, c->tmp_cell, 4ull * N)) return s;
     if (c->has_grid) {
         for (int b = 0; b < 2; ++b) {
-            if (bt_status s = ensure(c, c->sorted_rec[b], 16ull * N)) return s;
+            if (bt_status s = ensure(c, c->sorted_rec[b], 8ull * N)) return s;
             if (bt_status s = ensure(c, c->sorted_tag[b], 4ull * N)) return s;
         }
         if (bt_status s = ensure(c, c->slot_prefix, 16ull * (N + 1ull))) return s;
@@ -801,7 +801,7 @@ bt_status bt::upload_adapt(bt_ctx* c) {
     c->grid = g;
     c->cells = cells;
     stage_begin(c, "graph.rebin");
-    bt::launch_rebin(c->sorted_rec[c->cur].as<uint4>(), c->sorted_tag[c->cur].as<uint32_t>(), c->samples, c->grid,
+    bt::launch_rebin(c->sorted_rec[c->cur].as<float2>(), c->sorted_tag[c->cur].as<uint32_t>(), c->samples, c->grid,
                      c->tmp_xy.as<float2>(), c->tmp_tag.as<uint32_t>(), c->tmp_cell.as<uint32_t>(),
                      c->hist.as<uint32_t>(), c->stream);
     stage_end(c);
@@ -833,7 +833,7 @@ bt_status bt::prepare_records(bt_ctx* c) {
     cudaSetDevice(c->device);
     if (bt_status s = ensure(c, c->records, 12ull * c->samples)) return s;
     if (c->has_grid) {
-        bt::launch_unsort_records(c->sorted_rec[c->cur].as<uint4>(), c->sorted_tag[c->cur].as<uint32_t>(),
+        bt::launch_unsort_records(c->sorted_rec[c->cur].as<float2>(), c->sorted_tag[c->cur].as<uint32_t>(),
                                   c->edge_ids.as<uint32_t>(), c->samples, c->records.as<uint32_t>(), c->stream);
     } else {
         bt::launch_records_from_sample_order(c->tmp_xy.as<float2>(), c->edge_ids.as<uint32_t>(), c->samples,
@@ -1053,7 +1053,7 @@ bt_status current_positions(bt_ctx* c, const float2** out) {
         return BT_OK;
     }
     if (bt_status s = ensure(c, c->current, 8ull * c->samples)) return s;
-    bt::launch_positions_from_slots(c->sorted_rec[c->cur].as<uint4>(), c->sorted_tag[c->cur].as<uint32_t>(),
+    bt::launch_positions_from_slots(c->sorted_rec[c->cur].as<float2>(), c->sorted_tag[c->cur].as<uint32_t>(),
                                     c->samples, c->current.as<float2>(), c->stream);
     *out = c->current.as<float2>();
     return BT_OK;
@@ -1118,7 +1118,7 @@ bt_status bt_read_cells(bt_ctx* c, uint32_t* dst, size_t count) {
     if (!c->has_grid) return fail(c, BT_ERR_NOT_CONFIGURED, "neighbor radius is not configured");
     if (!dst || count != c->samples) return fail(c, BT_ERR_INVALID, "cell buffer must hold one id per sample");
     if (bt_status s = ensure(c, c->records, 12ull * c->samples)) return s;
-    bt::launch_grid_cells(c->sorted_rec[c->cur].as<uint4>(), c->sorted_tag[c->cur].as<uint32_t>(), c->samples,
+    bt::launch_grid_cells(c->sorted_rec[c->cur].as<float2>(), c->sorted_tag[c->cur].as<uint32_t>(), c->samples,
                           c->grid, c->records.as<uint32_t>(), c->stream);
     return copy_out(c, dst, c->records.p, 4 * count);
 }

@@ -12,8 +12,10 @@
 // atomics — nor on how N(p) is enumerated:
 //   p' = p + f32(f64(sum_q Q(q) - |N| Q(p)) / (f64(|N|) * 2^30)).
 //
-// B200 layout: samples live in slot order as 16-byte records
-// {x, y, Q(x) + 2^30, Q(y) + 2^30}, sorted by search cell (each grid cell split
+// B200 layout: samples live in slot order as 8-byte position records (their
+// biased fixed-point values Q + 2^30 recomputed where a sum needs them: an
+// exact conversion, cheaper than moving 16-byte records through the
+// candidate loads), sorted by search cell (each grid cell split
 // into kx x ky search cells, search cells row-major over the whole map), so a
 // row of search cells [a, b] is one contiguous slot range. The cell table (a
 // scan of the search-cell populations) gives each cell's first slot, and the
@@ -47,14 +49,14 @@ __global__ void __launch_bounds__(256) scatter_kernel(ScatterArgs a) {
     dev::scatter_sample(a, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
-__global__ void unsort_records_kernel(const uint4* rec, const uint32_t* tag, const uint32_t* edge_ids, uint32_t n,
+__global__ void unsort_records_kernel(const float2* rec, const uint32_t* tag, const uint32_t* edge_ids, uint32_t n,
                                       uint32_t* records) {
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n) return;
     const uint32_t i = tag[s] & ~kMovableBit;
-    const uint4 r = rec[s];
-    records[3 * static_cast<size_t>(i)] = r.x;
-    records[3 * static_cast<size_t>(i) + 1] = r.y;
+    const float2 r = rec[s];
+    records[3 * static_cast<size_t>(i)] = __float_as_uint(r.x);
+    records[3 * static_cast<size_t>(i) + 1] = __float_as_uint(r.y);
     records[3 * static_cast<size_t>(i) + 2] = edge_ids[i];
 }
 
@@ -74,12 +76,12 @@ __global__ void records_kernel(const float2* xy, const uint32_t* edge_ids, uint3
 }
 
 // cell_index (spatial_grid.wgsl:67-70) of each sample, sample order.
-__global__ void grid_cells_kernel(const uint4* rec, const uint32_t* tag, uint32_t n, Grid g, uint32_t* out) {
+__global__ void grid_cells_kernel(const float2* rec, const uint32_t* tag, uint32_t n, Grid g, uint32_t* out) {
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n) return;
-    const uint4 r = rec[s];
-    const uint32_t cx = grid_of(texel_of(__uint_as_float(r.x), g.map.wm1), g.rf, g.gw);
-    const uint32_t cy = grid_of(texel_of(__uint_as_float(r.y), g.map.hm1), g.rf, g.gh);
+    const float2 r = rec[s];
+    const uint32_t cx = grid_of(texel_of(r.x, g.map.wm1), g.rf, g.gw);
+    const uint32_t cy = grid_of(texel_of(r.y, g.map.hm1), g.rf, g.gh);
     out[tag[s] & ~kMovableBit] = cy * g.gw + cx;
 }
 
@@ -115,12 +117,11 @@ __global__ void __launch_bounds__(256) grid_pairs_kernel(const uint32_t* counts,
     }
 }
 
-__global__ void __launch_bounds__(256) rebin_kernel(const uint4* rec, const uint32_t* tag, uint32_t n, Grid g,
+__global__ void __launch_bounds__(256) rebin_kernel(const float2* rec, const uint32_t* tag, uint32_t n, Grid g,
                                                     float2* xy, uint32_t* out_tag, uint32_t* cell, uint32_t* hist) {
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     const bool valid = s < n;
-    const uint4 r = valid ? rec[s] : make_uint4(0u, 0u, 0u, 0u);
-    const float2 p = make_float2(__uint_as_float(r.x), __uint_as_float(r.y));
+    const float2 p = valid ? rec[s] : make_float2(0.0f, 0.0f);
     const uint32_t c = valid ? search_cell(p, g) : 0xFFFFFFFFu;
     const unsigned peers = __match_any_sync(0xFFFFFFFFu, c);
     if (!valid) return;
@@ -130,11 +131,10 @@ __global__ void __launch_bounds__(256) rebin_kernel(const uint4* rec, const uint
     cell[s] = c;
 }
 
-__global__ void positions_kernel(const uint4* rec, const uint32_t* tag, uint32_t n, float2* out) {
+__global__ void positions_kernel(const float2* rec, const uint32_t* tag, uint32_t n, float2* out) {
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n) return;
-    const uint4 r = rec[s];
-    out[tag[s] & ~kMovableBit] = make_float2(__uint_as_float(r.x), __uint_as_float(r.y));
+    out[tag[s] & ~kMovableBit] = rec[s];
 }
 
 }  // namespace
@@ -156,7 +156,7 @@ void launch_cell_table(const uint32_t* hist, size_t cells, uint32_t* cell_start,
                                        hist_tiles, s);
 }
 
-void launch_slot_prefix(const uint4* rec, uint32_t n, LL2* prefix, LL2* prefix_tiles, cudaStream_t s) {
+void launch_slot_prefix(const float2* rec, uint32_t n, LL2* prefix, LL2* prefix_tiles, cudaStream_t s) {
     reduce_tiles<LL2>(dev::RecordQSource{rec}, n, prefix_tiles, s);
     exclusive_scan_presummed<LL2>(dev::RecordQSource{rec}, ArraySink<LL2>{prefix}, n, prefix_tiles, s);
 }
@@ -171,13 +171,13 @@ void launch_grid_pairs(const uint32_t* hist, const Grid& g, uint32_t* scratch, u
     grid_pairs_kernel<<<std::min(div_up(grid_cells, 256), 1184u), 256, 0, s>>>(scratch, grid_cells, out);
 }
 
-void launch_rebin(const uint4* rec, const uint32_t* tag, uint32_t n, const Grid& g, float2* xy, uint32_t* out_tag,
+void launch_rebin(const float2* rec, const uint32_t* tag, uint32_t n, const Grid& g, float2* xy, uint32_t* out_tag,
                   uint32_t* cell, uint32_t* hist, cudaStream_t s) {
     if (n == 0) return;
     rebin_kernel<<<div_up(n, 256), 256, 0, s>>>(rec, tag, n, g, xy, out_tag, cell, hist);
 }
 
-void launch_unsort_records(const uint4* rec, const uint32_t* tag, const uint32_t* edge_ids, uint32_t n,
+void launch_unsort_records(const float2* rec, const uint32_t* tag, const uint32_t* edge_ids, uint32_t n,
                            uint32_t* records, cudaStream_t s) {
     if (n == 0) return;
     unsort_records_kernel<<<div_up(n, 256), 256, 0, s>>>(rec, tag, edge_ids, n, records);
@@ -194,13 +194,13 @@ void launch_records_from_sample_order(const float2* xy, const uint32_t* edge_ids
     records_kernel<<<div_up(n, 256), 256, 0, s>>>(xy, edge_ids, n, records);
 }
 
-void launch_grid_cells(const uint4* rec, const uint32_t* tag, uint32_t n, const Grid& g, uint32_t* out,
+void launch_grid_cells(const float2* rec, const uint32_t* tag, uint32_t n, const Grid& g, uint32_t* out,
                        cudaStream_t s) {
     if (n == 0) return;
     grid_cells_kernel<<<div_up(n, 256), 256, 0, s>>>(rec, tag, n, g, out);
 }
 
-void launch_positions_from_slots(const uint4* rec, const uint32_t* tag, uint32_t n, float2* out, cudaStream_t s) {
+void launch_positions_from_slots(const float2* rec, const uint32_t* tag, uint32_t n, float2* out, cudaStream_t s) {
     if (n == 0) return;
     positions_kernel<<<div_up(n, 256), 256, 0, s>>>(rec, tag, n, out);
 }

@@ -27,18 +27,18 @@ struct Acc {
 };
 
 // Exact test of every sample in slots [b, e) (neighbor_mean.wgsl:193-198).
-__device__ __forceinline__ void scan_range(const uint4* __restrict__ rec, uint32_t b, uint32_t e, float2 neg_p,
+__device__ __forceinline__ void scan_range(const float2* __restrict__ rec, uint32_t b, uint32_t e, float2 neg_p,
                                            float2 ts, float r2, Acc& acc) {
-#pragma unroll 4
+#pragma unroll 8
     for (uint32_t j = b; j < e; ++j) {
-        const uint4 q = __ldg(rec + j);
-        const float2 d = __fadd2_rn(make_float2(__uint_as_float(q.x), __uint_as_float(q.y)), neg_p);
+        const float2 q = __ldg(rec + j);
+        const float2 d = __fadd2_rn(q, neg_p);
         const float2 t = __fmul2_rn(d, ts);
         const float2 t2 = __fmul2_rn(t, t);
         const float d2 = t2.x + t2.y;
         if (d2 <= r2) {
-            acc.sx += q.z;
-            acc.sy += q.w;
+            acc.sx += biased_fixed(q.x);
+            acc.sy += biased_fixed(q.y);
             acc.count += 1u;
         }
     }
@@ -49,8 +49,7 @@ __device__ __forceinline__ void scan_range(const uint4* __restrict__ rec, uint32
 __device__ __forceinline__ void mean_sample(const MeanArgs& a, uint32_t i) {
     const bool valid = i < a.n;
     const Grid& g = a.g;
-    const uint4 me = valid ? a.rec[i] : make_uint4(0u, 0u, 0u, 0u);
-    const float2 p = make_float2(__uint_as_float(me.x), __uint_as_float(me.y));
+    const float2 p = valid ? a.rec[i] : make_float2(0.0f, 0.0f);
     const uint32_t tag = valid ? a.tag[i] : 0u;
     float2 np = p;
     uint32_t count = 0;
@@ -114,8 +113,8 @@ __device__ __forceinline__ void mean_sample(const MeanArgs& a, uint32_t i) {
         }
         count = acc.count;
         // Biased sums: sum (Q(q) + B) - n (Q(p) + B) = sum Q(q) - n Q(p).
-        const long long dx = static_cast<long long>(acc.sx - static_cast<unsigned long long>(count) * me.z);
-        const long long dy = static_cast<long long>(acc.sy - static_cast<unsigned long long>(count) * me.w);
+        const long long dx = static_cast<long long>(acc.sx - static_cast<unsigned long long>(count) * biased_fixed(p.x));
+        const long long dy = static_cast<long long>(acc.sy - static_cast<unsigned long long>(count) * biased_fixed(p.y));
         const double den = static_cast<double>(count) * 1073741824.0;
         np.x = p.x + static_cast<float>(static_cast<double>(dx) / den);
         np.y = p.y + static_cast<float>(static_cast<double>(dy) / den);
@@ -166,16 +165,16 @@ __device__ __forceinline__ void scatter_sample(const ScatterArgs& a, uint32_t i)
     }
     if (!ok) return;
     const float2 p = a.xy[i];
-    a.out_rec[slot] = make_uint4(__float_as_uint(p.x), __float_as_uint(p.y), biased_fixed(p.x), biased_fixed(p.y));
+    a.out_rec[slot] = p;
     a.out_tag[slot] = a.tag[i];
 }
 
 // Slot-prefix scan input: the biased fixed-point position of a record.
 struct RecordQSource {
-    const uint4* rec;
+    const float2* rec;
     __device__ __forceinline__ LL2 read(size_t j) const {
-        const uint4 r = rec[j];
-        return LL2{static_cast<long long>(r.z), static_cast<long long>(r.w)};
+        const float2 r = rec[j];
+        return LL2{static_cast<long long>(biased_fixed(r.x)), static_cast<long long>(biased_fixed(r.y))};
     }
     __device__ __forceinline__ void consume(size_t) const {}
 };

@@ -69,8 +69,9 @@ void launch_blur_vertical(const float* in, float* out, uint32_t w, uint32_t h, c
 void launch_normalize(const float* in, const uint32_t* peak, float* out, size_t n, cudaStream_t s);
 
 // ---- neighbour grid and mean (grid.cu) ----
-// Slot-order sample record: {f32 x bits, f32 y bits, Qx + 2^30, Qy + 2^30}
-// with Q(v) = round-half-even(v * 2^30), so the biased values are unsigned.
+// Slot-order sample records hold the position alone (float2, 8 bytes); the
+// exact neighbour sums use Q(v) = round-half-even(v * 2^30), recomputed from
+// it and biased by 2^30 so that the values are unsigned.
 constexpr uint32_t kFixedBias = 1u << 30;
 
 __device__ __forceinline__ uint32_t biased_fixed(float v) {
@@ -83,7 +84,7 @@ enum SearchMode : int {
 };
 
 struct MeanArgs {
-    const uint4* rec;        // slot order (sorted by search cell)
+    const float2* rec;       // slot order (sorted by search cell)
     const uint32_t* tag;     // sample index | movable bit, slot order
     const uint32_t* cell_start;   // cell table: first slot of each search cell (cells + 1)
     const LL2* prefix;       // sum of the biased positions of all earlier slots (n + 1)
@@ -121,13 +122,13 @@ void launch_grid_pairs(const uint32_t* hist, const Grid& g, uint32_t* scratch, u
 // Re-bins slot-order records under another search-cell shape: positions,
 // tags and new search cells in slot order (the scatter's input) and the new
 // populations (hist must be zero).
-void launch_rebin(const uint4* rec, const uint32_t* tag, uint32_t n, const Grid& g, float2* xy, uint32_t* out_tag,
+void launch_rebin(const float2* rec, const uint32_t* tag, uint32_t n, const Grid& g, float2* xy, uint32_t* out_tag,
                   uint32_t* cell, uint32_t* hist, cudaStream_t s);
 
 // Slot prefix of the scattered records: prefix[j] = sum over slots < j of the
 // biased fixed-point positions (n + 1 entries); prefix_tiles (scan_tiles(n) +
 // 1 entries) is its scratch.
-void launch_slot_prefix(const uint4* rec, uint32_t n, LL2* prefix, LL2* prefix_tiles, cudaStream_t s);
+void launch_slot_prefix(const float2* rec, uint32_t n, LL2* prefix, LL2* prefix_tiles, cudaStream_t s);
 
 struct ScatterArgs {
     const float2* xy;
@@ -135,7 +136,7 @@ struct ScatterArgs {
     const uint32_t* cell;
     const uint32_t* cell_start;
     uint32_t* hist;          // counted down to zero
-    uint4* out_rec;
+    float2* out_rec;
     uint32_t* out_tag;
     uint32_t n;
     uint32_t cells;          // search cells
@@ -144,14 +145,14 @@ struct ScatterArgs {
 void launch_scatter(const ScatterArgs& a, cudaStream_t s);
 
 // Sample-order records {x, y, edge_id} from slot order.
-void launch_unsort_records(const uint4* rec, const uint32_t* tag, const uint32_t* edge_ids, uint32_t n,
+void launch_unsort_records(const float2* rec, const uint32_t* tag, const uint32_t* edge_ids, uint32_t n,
                            uint32_t* records, cudaStream_t s);
 void launch_unsort_u32(const uint32_t* values, const uint32_t* tag, uint32_t n, uint32_t* out, cudaStream_t s);
 void launch_records_from_sample_order(const float2* xy, const uint32_t* edge_ids, uint32_t n, uint32_t* records,
                                       cudaStream_t s);
-void launch_grid_cells(const uint4* rec, const uint32_t* tag, uint32_t n, const Grid& g, uint32_t* out,
+void launch_grid_cells(const float2* rec, const uint32_t* tag, uint32_t n, const Grid& g, uint32_t* out,
                        cudaStream_t s);
-void launch_positions_from_slots(const uint4* rec, const uint32_t* tag, uint32_t n, float2* out, cudaStream_t s);
+void launch_positions_from_slots(const float2* rec, const uint32_t* tag, uint32_t n, float2* out, cudaStream_t s);
 
 // ---- distortion (distortion.cu) ----
 // Per-edge squared_integral of original vs current (sample order); status bit
