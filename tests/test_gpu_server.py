@@ -145,3 +145,23 @@ def test_invalid_request_fails_without_stopping_the_server():
     with pytest.raises(bt.BtError):
         server.next(0.05)                  # nothing left
     server.close()
+
+
+def test_served_result_renders_like_a_standalone_run():
+    # A finished request's context can be drawn (bt_render) before release.
+    w = synthetic.small()
+    o = options(w, endpoint_dots=True, palette=2)
+    server = bt.Server(max_active=4)
+    rid = server.submit(o, w.xy, w.starts, 3)
+    r = server.next(60.0)
+    assert r.status == 0 and r.id == rid, r.message
+    frame = server.result(rid).render()
+    g = bt.Gpu(o)
+    g.upload((w.xy, w.starts))
+    g.iterate(3)
+    ref = g.render()
+    g.close()
+    assert frame.colored_pixels == ref.colored_pixels > 0
+    np.testing.assert_array_equal(frame.rgba, ref.rgba)
+    server.release(rid)
+    server.close()
