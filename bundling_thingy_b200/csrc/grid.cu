@@ -39,9 +39,11 @@
 namespace bt {
 namespace {
 
-// Six resident 256-thread CTAs per SM (at most 42 registers) hide more of
-// the cell-table and record load latency than five.
-__global__ void __launch_bounds__(256, 6) neighbor_mean_kernel(MeanArgs a) {
+// Five resident 256-thread CTAs per SM (at most 48 registers): with 8-byte
+// records and eight candidate loads in flight per lane, the registers are
+// worth more than a sixth CTA (0.86 against 0.90 ms per steady-state
+// iteration of the large workload; four CTAs: 0.92).
+__global__ void __launch_bounds__(256, 5) neighbor_mean_kernel(MeanArgs a) {
     dev::mean_sample(a, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
