@@ -83,7 +83,7 @@ class _Info(ctypes.Structure):
 class _ServerOptions(ctypes.Structure):
     _fields_ = [
         ("device", ctypes.c_int32), ("max_active", ctypes.c_uint32), ("budget_bytes", ctypes.c_uint64),
-        ("max_step", ctypes.c_uint32), ("reserved0", ctypes.c_uint32), ("reserve_bytes", ctypes.c_uint64),
+        ("max_step", ctypes.c_uint32), ("solo_samples", ctypes.c_uint32), ("reserve_bytes", ctypes.c_uint64),
         ("reserved", ctypes.c_uint32 * 4),
     ]
 
@@ -663,11 +663,14 @@ class Server:
     iteration count is reached. Results stay on the device until released."""
 
     def __init__(self, device: int = 0, max_active: int = 32, budget_bytes: int = 120_000_000_000,
-                 max_step: int = 1, reserve_bytes: int = 0):
+                 max_step: int = 1, reserve_bytes: int = 0, solo_samples: int = 0):
+        """solo_samples: requests of at least this many samples iterate on
+        their own context beside the batch (0 = 32768; 2**32 - 1 = never)."""
         o = _ServerOptions()
         library().bt_server_options_init(ctypes.byref(o))
         o.device, o.max_active, o.budget_bytes, o.max_step = device, max_active, budget_bytes, max_step
         o.reserve_bytes = reserve_bytes
+        o.solo_samples = solo_samples
         h = _vp()
         _check(library().bt_server_create(ctypes.byref(o), ctypes.byref(h)))
         self._h = h

@@ -210,7 +210,10 @@ Budget on_budget(bt_server* s, const Request* r) {
     return Budget::Fail;
 }
 
-size_t active_count(const bt_server* s) { return s->uploading.size() + s->running.size(); }
+size_t active_count(const bt_server* s) { return s->uploading.size() + s->running.size() + s->finishing.size(); }
+
+// Samples from which a request iterates on its own (bt_server_options::solo_samples = 0).
+constexpr uint32_t kSoloSamples = 32768;
 
 // Records the end of the work queued so far on a context's stream.
 bool mark(bt_ctx* c) { return cudaEventRecord(c->done, c->stream) == cudaSuccess; }
@@ -348,6 +351,22 @@ bool advance_uploads(bt_server* s) {
         if (st != BT_OK) {
             const std::string msg = r->ctx->err;
             fail_request(s, r, st, msg);
+            continue;
+        }
+        const uint32_t solo = s->opt.solo_samples ? s->opt.solo_samples : kSoloSamples;
+        if (samples >= solo) {
+            // Large enough to fill the device by itself (a persistent batch
+            // step would only slow it down): all its iterations and the
+            // records on its own stream, beside the batch.
+            st = bt_iterate_async(r->ctx, r->iterations);
+            if (st == BT_OK) st = bt::prepare_records(r->ctx);
+            if (st == BT_OK && mark(r->ctx)) {
+                r->state = State::Running;
+                s->finishing.push_back(r);
+                continue;
+            }
+            const std::string msg = r->ctx->err;
+            fail_request(s, r, st ? st : BT_ERR_CUDA, msg);
             continue;
         }
         if (bt_status ast = bt::batch_attach(s->batch, r->ctx, &r->slot)) {

@@ -265,7 +265,9 @@ typedef struct bt_server_options {
     uint32_t max_active;      /* graphs uploading or iterating at once (0 = unlimited) */
     uint64_t budget_bytes;    /* device memory of all resident graphs and pooled contexts */
     uint32_t max_step;        /* batch iterations between admission points while requests wait to join (>= 1) */
-    uint32_t reserved0;
+    uint32_t solo_samples;    /* requests of at least this many samples fill the device alone: they iterate
+                                 on their own context's stream and CUDA graphs beside the batch instead of
+                                 joining it (0 = 32768; UINT32_MAX = every request joins the batch) */
     uint64_t reserve_bytes;   /* device memory mapped into the allocator's pool at creation, so that
                                  admissions do not map memory while steps run (0 = none; at most
                                  budget_bytes) */

@@ -64,8 +64,11 @@ def drain(server, n, expected, timeout=60.0):
     return seen
 
 
-def test_requests_in_the_mix_match_standalone_runs():
-    server = bt.Server(max_active=8)
+@pytest.mark.parametrize("solo_samples", [0, 1, 2**32 - 1])
+def test_requests_in_the_mix_match_standalone_runs(solo_samples):
+    # Default threshold (the larger requests iterate on their own contexts),
+    # every request on its own, every request in the batch.
+    server = bt.Server(max_active=8, solo_samples=solo_samples)
     t0 = server.clock() + 0.01
     expected = {}
     for i, (w, o, iters) in enumerate(mixed_requests()):
