@@ -152,6 +152,7 @@ SIGNATURES = {
     "bt_batch_synchronize": ([_vp], ctypes.c_int32),
     "bt_batch_iterate_timed": ([_vp, ctypes.c_uint32, _f32p], ctypes.c_int32),
     "bt_batch_slot_count": ([_vp, _u32p, _u32p], ctypes.c_int32),
+    "bt_batch_set_solo_samples": ([_vp, ctypes.c_uint32], ctypes.c_int32),
     "bt_batch_slot": ([_vp, ctypes.c_uint32], _vp),
     "bt_server_options_init": ([ctypes.POINTER(_ServerOptions)], None),
     "bt_server_create": ([ctypes.POINTER(_ServerOptions), ctypes.POINTER(_vp)], ctypes.c_int32),
@@ -554,11 +555,20 @@ class Batch:
     a graph x tile work queue (bt_batch_*). Each slot keeps its own options;
     its results equal a single-graph :class:`Gpu` run bit for bit."""
 
-    def __init__(self, device: int = 0):
+    def __init__(self, device: int = 0, solo_samples: int = 0):
+        """solo_samples: slots of at least this many samples iterate on their
+        own context beside the persistent step (0 = never, the default)."""
         h = _vp()
         _check(library().bt_batch_create(device, ctypes.byref(h)))
         self._h = h
         self._options: dict[int, Options] = {}
+        if solo_samples:
+            self.set_solo_samples(solo_samples)
+
+    def set_solo_samples(self, samples: int) -> None:
+        """bt_batch_set_solo_samples: the slot size from which slots iterate on
+        their own context (0 = never); from the next step."""
+        self._ck(library().bt_batch_set_solo_samples(self._h, samples))
 
     def close(self) -> None:
         h = getattr(self, "_h", None)

@@ -274,9 +274,16 @@ __global__ void batch_advance_kernel(BatchArgs b) {
     }
 }
 
+// Slots of at least bt_batch::solo_samples samples iterate on their own
+// context's stream and CUDA graphs, beside the persistent step, instead of
+// joining its work lists (opt-in: large dense graphs run the single-graph
+// kernels faster, while mid-size graphs on small maps do better in the step).
+constexpr uint32_t kNeverSolo = UINT32_MAX;
+
 struct Slot {
     bt_ctx* ctx = nullptr;
     bool active = false;
+    bool solo = false;       // iterates on its own context (not in the work lists)
     DevBuf taps;             // Taps per density pass
     uint32_t taps_count = 0;
     uint32_t taps_first_pass = 0;   // taps[i] is pass i (tables start at pass 0)
@@ -290,6 +297,7 @@ struct bt_batch {
     int sms = 148;
     cudaStream_t stream = nullptr;
     cudaEvent_t done = nullptr, t0 = nullptr, t1 = nullptr;
+    cudaEvent_t fork = nullptr;   // start of a step, for the solo slots' streams
     std::string err;
     std::vector<bt::Slot> slots;
     bt::DevBuf descs, state, counts, counters, status, lists[bt::kLists];
@@ -300,6 +308,7 @@ struct bt_batch {
     size_t blur_smem = 0;
     uint32_t* h_status = nullptr;
     uint32_t max_pass = 0;     // highest density pass the taps tables cover
+    uint32_t solo_samples = bt::kNeverSolo;
 };
 
 namespace bt {
@@ -339,6 +348,14 @@ bt_status bgrow(bt_batch* b, DevBuf& buf, size_t bytes) {
 }
 
 bt_status bwait(bt_batch* b) {
+    // The batch stream already waits for the solo slots' queued work after
+    // each step; work queued on them since (a re-upload) is joined here.
+    for (const Slot& s : b->slots) {
+        if (!s.active || !s.solo) continue;
+        cudaError_t j = cudaEventRecord(s.ctx->done, s.ctx->stream);
+        if (j == cudaSuccess) j = cudaStreamWaitEvent(b->stream, s.ctx->done, 0);
+        if (j != cudaSuccess) return bcuda(b, j, "stream ordering");
+    }
     cudaError_t e = cudaEventRecord(b->done, b->stream);
     if (e != cudaSuccess) return bcuda(b, e, "cudaEventRecord");
     const auto start = std::chrono::steady_clock::now();
@@ -446,7 +463,7 @@ bt_status rebuild(bt_batch* b) {
     for (size_t i = 0; i < n; ++i) {
         Slot& s = b->slots[i];
         std::memset(&descs[i], 0, sizeof(SlotDesc));
-        if (!s.active) continue;
+        if (!s.active || s.solo) continue;
         bt_ctx* c = s.ctx;
         if (bt_status st = fill_taps(b, s, std::max(b->max_pass, c->density_passes) + kTapsHorizon)) return st;
         const uint32_t cell_tiles = static_cast<uint32_t>(scan_tiles<uint32_t>(c->cells));
@@ -528,7 +545,7 @@ bt_status rebuild(bt_batch* b) {
 // iterations (all active slots advance together).
 void advance_hosts(bt_batch* b, uint32_t n) {
     for (Slot& s : b->slots) {
-        if (!s.active) continue;
+        if (!s.active || s.solo) continue;   // solo contexts keep their own counts
         bt_ctx* c = s.ctx;
         c->cur ^= static_cast<int>(n & 1u);
         c->iterations += n;
@@ -565,6 +582,7 @@ bt_status batch_attach(bt_batch* b, bt_ctx* c, uint32_t* slot) {
     if (s.ctx) bt_destroy(s.ctx);
     s.ctx = c;
     s.active = true;
+    s.solo = c->samples >= b->solo_samples;
     s.taps_count = 0;
     b->dirty = true;
     *slot = idx;
@@ -641,6 +659,8 @@ bt_status bt_batch_create(int32_t device, bt_batch** out) {
     }
     if ((e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking)) != cudaSuccess)
         return bail(bcuda(b, e, "cudaStreamCreate"));
+    if ((e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming)) != cudaSuccess)
+        return bail(bcuda(b, e, "cudaEventCreate"));
     if ((e = cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming)) != cudaSuccess)
         return bail(bcuda(b, e, "cudaEventCreate"));
     if ((e = cudaEventCreate(&b->t0)) != cudaSuccess || (e = cudaEventCreate(&b->t1)) != cudaSuccess)
@@ -671,6 +691,7 @@ void bt_batch_destroy(bt_batch* b) {
     if (b->stream) cudaStreamSynchronize(b->stream);   // the frees above
     if (b->h_status) cudaFreeHost(b->h_status);
     if (b->done) cudaEventDestroy(b->done);
+    if (b->fork) cudaEventDestroy(b->fork);
     if (b->t0) cudaEventDestroy(b->t0);
     if (b->t1) cudaEventDestroy(b->t1);
     if (b->stream) cudaStreamDestroy(b->stream);
@@ -753,20 +774,42 @@ bt_status bt_batch_remove(bt_batch* b, uint32_t slot) {
 bt_status bt_batch_iterate_async(bt_batch* b, uint32_t n) {
     if (!b) return bfail(nullptr, BT_ERR_INVALID, "null batch");
     cudaSetDevice(b->device);
-    bool any = false;
+    bool any = false, any_solo = false;
     uint32_t reach = 0;
     for (Slot& s : b->slots) {
         if (!s.active) continue;
+        if (s.solo) {
+            any_solo = true;
+            continue;
+        }
         any = true;
         reach = std::max(reach, s.ctx->density_passes + n);
         if (s.taps_count > 1 && reach >= s.taps_count) b->dirty = true;   // extend shrinking-σ tables
     }
-    if (!any) return BT_OK;
-    b->max_pass = std::max(b->max_pass, reach);
-    if (b->dirty)
-        if (bt_status s = rebuild(b)) return s;
-    for (uint32_t i = 0; i < n; ++i) BB_CUDA(b, cudaGraphLaunch(b->graph, b->stream));
-    advance_hosts(b, n);
+    if (any_solo && n > 0) {
+        // Solo slots start after the batch's earlier work and run beside
+        // this step; the batch stream waits for them after its own launches.
+        BB_CUDA(b, cudaEventRecord(b->fork, b->stream));
+        for (Slot& s : b->slots) {
+            if (!s.active || !s.solo) continue;
+            BB_CUDA(b, cudaStreamWaitEvent(s.ctx->stream, b->fork, 0));
+            if (bt_status st = bt_iterate_async(s.ctx, n)) return bfail(b, st, s.ctx->err);
+        }
+    }
+    if (any) {
+        b->max_pass = std::max(b->max_pass, reach);
+        if (b->dirty)
+            if (bt_status s = rebuild(b)) return s;
+        for (uint32_t i = 0; i < n; ++i) BB_CUDA(b, cudaGraphLaunch(b->graph, b->stream));
+        advance_hosts(b, n);
+    }
+    if (any_solo && n > 0) {
+        for (Slot& s : b->slots) {
+            if (!s.active || !s.solo) continue;
+            BB_CUDA(b, cudaEventRecord(s.ctx->done, s.ctx->stream));
+            BB_CUDA(b, cudaStreamWaitEvent(b->stream, s.ctx->done, 0));
+        }
+    }
     return BT_OK;
 }
 
@@ -775,6 +818,11 @@ bt_status bt_batch_synchronize(bt_batch* b) {
     cudaSetDevice(b->device);
     if (bt_status s = bwait(b)) return s;
     BB_CUDA(b, cudaMemcpy(b->h_status, b->status.p, 4, cudaMemcpyDeviceToHost));
+    for (const Slot& s : b->slots) {
+        if (!s.active || !s.solo) continue;
+        BB_CUDA(b, cudaMemcpy(b->h_status + 1, s.ctx->status.p, 4, cudaMemcpyDeviceToHost));
+        b->h_status[0] |= b->h_status[1];
+    }
     if (b->h_status[0] & 8u) return bfail(b, BT_ERR_CUDA, "inconsistent neighbour-grid binning");
     return BT_OK;
 }
@@ -794,6 +842,17 @@ bt_status bt_batch_iterate_timed(bt_batch* b, uint32_t n, float* device_ms) {
     BB_CUDA(b, cudaEventRecord(b->t1, b->stream));
     if (bt_status s = bt_batch_synchronize(b)) return s;
     BB_CUDA(b, cudaEventElapsedTime(device_ms, b->t0, b->t1));
+    return BT_OK;
+}
+
+bt_status bt_batch_set_solo_samples(bt_batch* b, uint32_t samples) {
+    if (!b) return bfail(nullptr, BT_ERR_INVALID, "null batch");
+    cudaSetDevice(b->device);
+    if (bt_status s = bwait(b)) return s;   // no step in flight while slots change lanes
+    b->solo_samples = samples ? samples : kNeverSolo;
+    for (Slot& s : b->slots)
+        if (s.active) s.solo = s.ctx->samples >= b->solo_samples;
+    b->dirty = true;
     return BT_OK;
 }
 

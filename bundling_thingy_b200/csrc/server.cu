@@ -569,6 +569,9 @@ bt_status bt_server_create(const bt_server_options* options, bt_server** out) {
         delete s;
         return sfail(nullptr, st, msg);
     }
+    // The server picks each request's lane itself (solo_samples): whatever
+    // it attaches stays in the persistent step.
+    bt_batch_set_solo_samples(s->batch, UINT32_MAX);
     if (cudaEventCreateWithFlags(&s->step_done, cudaEventDisableTiming) != cudaSuccess) {
         bt_batch_destroy(s->batch);
         delete s;

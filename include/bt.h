@@ -238,6 +238,13 @@ bt_status bt_batch_synchronize(bt_batch* batch);
 /* bt_batch_iterate with the device milliseconds of the n iterations. */
 bt_status bt_batch_iterate_timed(bt_batch* batch, uint32_t n, float* device_ms);
 bt_status bt_batch_slot_count(bt_batch* batch, uint32_t* active, uint32_t* capacity);
+/* Slots of at least `samples` samples iterate on their own context's stream
+ * and CUDA graphs, beside the persistent step and concurrently with it,
+ * instead of joining its work lists (0 or UINT32_MAX = every slot joins, the
+ * default). Large dense graphs run faster that way; mid-size graphs on small
+ * maps run faster in the step. Applies to every slot from the next
+ * iteration; results are the same either way. */
+bt_status bt_batch_set_solo_samples(bt_batch* batch, uint32_t samples);
 /* The context of a slot, for the bt_read_* and bt_get_info calls; owned by
  * the batch (do not destroy or iterate it). Waits for the batch's work. */
 bt_ctx* bt_batch_slot(bt_batch* batch, uint32_t slot);

@@ -40,6 +40,12 @@ def mixed_jobs():
     ]
 
 
+# Every slot in the persistent step (the default, the engine under test), or
+# every slot on its own context.
+PERSISTENT = 2**32 - 1
+POLICIES = [PERSISTENT, 1]
+
+
 def standalone(w, o, iterations):
     g = bt.Gpu(o)
     g.upload((w.xy, w.starts))
@@ -60,9 +66,10 @@ def check_slot(batch, slot, expected):
         np.testing.assert_array_equal(view.read_density(), expected[2])
 
 
-def test_mixed_batch_matches_standalone_runs():
+@pytest.mark.parametrize("solo_samples", POLICIES)
+def test_mixed_batch_matches_standalone_runs(solo_samples):
     jobs = mixed_jobs()
-    batch = bt.Batch()
+    batch = bt.Batch(solo_samples=solo_samples)
     slots = [batch.add(o, w.xy, w.starts)[0] for w, o in jobs]
     assert batch.active() == len(jobs)
     batch.iterate(3)
@@ -78,7 +85,7 @@ def test_mixed_batch_matches_standalone_runs():
 def test_first_slot_matches_oracle(oracle):
     w = synthetic.small()
     o = workload_options(w)
-    batch = bt.Batch()
+    batch = bt.Batch(solo_samples=PERSISTENT)
     slot, n = batch.add(o, w.xy, w.starts)
     batch.add(*(lambda m: (workload_options(m), m.xy, m.starts))(synthetic.mid()))
     batch.iterate(4)
@@ -92,9 +99,11 @@ def test_first_slot_matches_oracle(oracle):
     np.testing.assert_array_equal(batch.slot(slot).read_density(), ora.normalized())
 
 
-def test_slots_join_and_leave_between_iterations():
+@pytest.mark.parametrize("solo_samples", POLICIES + [200000])
+def test_slots_join_and_leave_between_iterations(solo_samples):
+    # 200000: the small graphs in the persistent step, the mid one on its own.
     jobs = mixed_jobs()
-    batch = bt.Batch()
+    batch = bt.Batch(solo_samples=solo_samples)
     a = batch.add(jobs[0][1], jobs[0][0].xy, jobs[0][0].starts)[0]
     b = batch.add(jobs[1][1], jobs[1][0].xy, jobs[1][0].starts)[0]
     batch.iterate(1)                       # a, b at parity 1
@@ -112,7 +121,7 @@ def test_slots_join_and_leave_between_iterations():
 def test_long_shrinking_sigma_run_extends_taps():
     w = synthetic.small()
     o = workload_options(w)
-    batch = bt.Batch()
+    batch = bt.Batch(solo_samples=PERSISTENT)
     slot = batch.add(o, w.xy, w.starts)[0]
     batch.iterate(70)                      # beyond the precomputed taps horizon
     check_slot(batch, slot, standalone(w, o, 70))
@@ -132,7 +141,7 @@ def test_batch_errors():
 
 def test_add_many_uploads_concurrently_and_matches_standalone():
     jobs = mixed_jobs()
-    batch = bt.Batch()
+    batch = bt.Batch(solo_samples=PERSISTENT)
     added = batch.add_many([(o, w.xy, w.starts) for w, o in jobs])
     assert [s for s, _ in added] == list(range(len(jobs)))
     for (w, o), (slot, n) in zip(jobs, added):
@@ -147,7 +156,7 @@ def test_add_many_is_all_or_nothing():
     o = workload_options(w)
     bad = w.starts.copy()
     bad[-1] = w.xy.shape[0] + 5            # last start past the point count
-    batch = bt.Batch()
+    batch = bt.Batch(solo_samples=PERSISTENT)
     batch.add(o, w.xy, w.starts)
     with pytest.raises(bt.BtError) as e:
         batch.add_many([(o, w.xy, w.starts), (o, w.xy, bad)])
@@ -155,3 +164,18 @@ def test_add_many_is_all_or_nothing():
     assert batch.active() == 1
     batch.iterate(1)
     check_slot(batch, 0, standalone(w, o, 1))
+
+
+def test_slots_change_lanes_between_iterations():
+    # The same graphs moved between the persistent step and their own
+    # contexts mid-run: results still equal standalone runs.
+    jobs = mixed_jobs()[:3]
+    batch = bt.Batch(solo_samples=PERSISTENT)
+    slots = [batch.add(o, w.xy, w.starts)[0] for w, o in jobs]
+    batch.iterate(2)
+    batch.set_solo_samples(1)
+    batch.iterate(2)
+    batch.set_solo_samples(PERSISTENT)
+    batch.iterate(1)
+    for (w, o), slot in zip(jobs, slots):
+        check_slot(batch, slot, standalone(w, o, 5))
