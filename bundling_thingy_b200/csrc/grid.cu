@@ -39,11 +39,13 @@
 namespace bt {
 namespace {
 
-// Five resident 256-thread CTAs per SM (at most 48 registers): with 8-byte
-// records and eight candidate loads in flight per lane, the registers are
-// worth more than a sixth CTA (0.86 against 0.90 ms per steady-state
-// iteration of the large workload; four CTAs: 0.92).
-__global__ void __launch_bounds__(256, 5) neighbor_mean_kernel(MeanArgs a) {
+// Forty resident warps per SM at 48 registers: with 8-byte records and eight
+// candidate loads in flight per lane, the registers are worth more than a
+// sixth 256-thread CTA (0.86 against 0.90 ms per steady-state iteration of
+// the large workload; four: 0.92). Ten CTAs of 128 rather than five of 256:
+// samples of very different neighbourhood sizes share an SM at a finer
+// grain, which trims the tail (0.845 against 0.863 ms; 64 threads: 0.849).
+__global__ void __launch_bounds__(128, 10) neighbor_mean_kernel(MeanArgs a) {
     dev::mean_sample(a, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
@@ -143,7 +145,7 @@ __global__ void positions_kernel(const float2* rec, const uint32_t* tag, uint32_
 
 void launch_neighbor_mean(const MeanArgs& a, cudaStream_t s) {
     if (a.n == 0) return;
-    neighbor_mean_kernel<<<div_up(a.n, 256), 256, 0, s>>>(a);
+    neighbor_mean_kernel<<<div_up(a.n, 128), 128, 0, s>>>(a);
 }
 
 void launch_scatter(const ScatterArgs& a, cudaStream_t s) {
