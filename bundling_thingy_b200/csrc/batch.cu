@@ -214,7 +214,7 @@ __device__ __forceinline__ const Taps& pass_taps(const BlurSlot& s, uint32_t pas
     return s.taps[pass < s.taps_count ? pass : s.taps_count - 1];
 }
 
-__global__ void __launch_bounds__(dev::kBlurThreads) batch_blur_h_kernel(BatchArgs b) {
+__global__ void __launch_bounds__(dev::kBlurThreads, dev::kBlurMinCtas) batch_blur_h_kernel(BatchArgs b) {
     extern __shared__ float smem[];
     __shared__ uint32_t t_sh;
     __shared__ int rp_sh;
@@ -232,7 +232,7 @@ __global__ void __launch_bounds__(dev::kBlurThreads) batch_blur_h_kernel(BatchAr
     }
 }
 
-__global__ void __launch_bounds__(dev::kBlurThreads) batch_blur_v_kernel(BatchArgs b) {
+__global__ void __launch_bounds__(dev::kBlurThreads, dev::kBlurMinCtas) batch_blur_v_kernel(BatchArgs b) {
     extern __shared__ float smem[];
     __shared__ uint32_t t_sh;
     __shared__ int rp_sh;

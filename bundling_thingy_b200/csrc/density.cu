@@ -24,7 +24,7 @@ using dev::kBlurLines;
 using dev::kBlurSpan;
 using dev::kBlurThreads;
 
-__global__ void __launch_bounds__(kBlurThreads) blur_h_kernel(const uint32_t* __restrict__ in, float* __restrict__ out,
+__global__ void __launch_bounds__(kBlurThreads, dev::kBlurMinCtas) blur_h_kernel(const uint32_t* __restrict__ in, float* __restrict__ out,
                                                               uint32_t W, uint32_t H, Taps taps_arg, int RP) {
     extern __shared__ float smem[];
     float* taps = smem;
@@ -33,7 +33,7 @@ __global__ void __launch_bounds__(kBlurThreads) blur_h_kernel(const uint32_t* __
     dev::blur_h_tile(in, out, W, H, taps, RP, blockIdx.x, blockIdx.y, tile);
 }
 
-__global__ void __launch_bounds__(kBlurThreads) blur_v_kernel(const float* __restrict__ in, float* __restrict__ out,
+__global__ void __launch_bounds__(kBlurThreads, dev::kBlurMinCtas) blur_v_kernel(const float* __restrict__ in, float* __restrict__ out,
                                                               uint32_t W, uint32_t H, Taps taps_arg, int RP,
                                                               uint32_t* peak) {
     extern __shared__ float smem[];

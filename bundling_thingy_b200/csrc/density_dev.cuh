@@ -13,6 +13,13 @@ constexpr int kBlurSegs = 16;                         // warps: 8 outputs each
 constexpr int kBlurOut = 8;
 constexpr int kBlurSpan = kBlurSegs * kBlurOut;       // outputs per line per CTA
 constexpr int kBlurThreads = kBlurLines * kBlurSegs;
+// Three resident CTAs per SM (40 registers): the staging loads of one CTA
+// overlap the arithmetic of the others. Unbounded, the kernels took 56-70
+// registers and ran two CTAs per SM, or one (the batch's vertical pass):
+// 13.1 against 11.9 ms per iteration of 256 mixed graphs in a batch. Only the
+// batch's horizontal pass spills (20 bytes); it ran no slower than a
+// spill-free variant with taps four at a time.
+constexpr int kBlurMinCtas = 3;
 
 __host__ __device__ inline int blur_padded(int R) { return (R + 7) & ~7; }
 
