@@ -123,18 +123,25 @@ __device__ __forceinline__ void mean_sample(const MeanArgs& a, uint32_t i) {
     // in one cell (neighbours in slot order mostly do) add their count once.
     const uint32_t c = valid ? search_cell(np, g) : 0xFFFFFFFFu;
     const unsigned peers = __match_any_sync(0xFFFFFFFFu, c);
+    const int lane = threadIdx.x & 31;
+    if (a.counts) {
+        // Density splat, warp-aggregated too: once bundled, the samples of a
+        // warp mostly share texels, and one add per texel spares the L2 the
+        // serialised same-address atomics (integer sums: the counts are the
+        // same in any order).
+        uint32_t d = 0xFFFFFFFFu;                          // stays so off the map
+        if (valid) splat_index(np.x, np.y, g.map, &d);
+        const unsigned same = __match_any_sync(0xFFFFFFFFu, d);
+        if (d != 0xFFFFFFFFu && lane == __ffs(same) - 1) atomicAdd(&a.counts[d], static_cast<uint32_t>(__popc(same)));
+    }
     if (!valid) return;
-    if ((threadIdx.x & 31) == __ffs(peers) - 1) {
+    if (lane == __ffs(peers) - 1) {
         atomicAdd(&a.hist[c], static_cast<uint32_t>(__popc(peers)));
         if (a.hist_tiles) atomicAdd(&a.hist_tiles[c / kCellTile], static_cast<uint32_t>(__popc(peers)));
     }
     a.out_xy[i] = np;
     a.out_tag[i] = tag;
     a.out_cell[i] = c;
-    if (a.counts) {
-        uint32_t d;
-        if (splat_index(np.x, np.y, g.map, &d)) atomicAdd(&a.counts[d], 1u);
-    }
     if (a.neighbors) a.neighbors[i] = count;
 }
 
