@@ -54,20 +54,30 @@ __device__ __forceinline__ bool movable(const uint32_t* __restrict__ ids, uint32
     return i > 0 && i + 1 < n && ids[i - 1] == ids[i] && ids[i + 1] == ids[i];
 }
 
+// Every lane of the grid's warps reaches the splat (idle lanes past n too):
+// it is warp-aggregated.
 __global__ void __launch_bounds__(256) advect_kernel(AdvectArgs a) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.n) return;
-    float2 out = a.xy[i];
-    if (movable(a.edge_ids, a.n, i)) {
-        const float2 s = advected(a, out);
-        const float2 p = movable(a.edge_ids, a.n, i - 1) ? advected(a, a.xy[i - 1]) : a.xy[i - 1];
-        const float2 q = movable(a.edge_ids, a.n, i + 1) ? advected(a, a.xy[i + 1]) : a.xy[i + 1];
-        out.x = __fadd_rn(s.x, __fmul_rn(a.smooth, __fsub_rn(__fmul_rn(__fadd_rn(p.x, q.x), 0.5f), s.x)));
-        out.y = __fadd_rn(s.y, __fmul_rn(a.smooth, __fsub_rn(__fmul_rn(__fadd_rn(p.y, q.y), 0.5f), s.y)));
+    uint32_t d = 0xFFFFFFFFu;                              // no texel
+    if (i < a.n) {
+        float2 out = a.xy[i];
+        if (movable(a.edge_ids, a.n, i)) {
+            const float2 s = advected(a, out);
+            const float2 p = movable(a.edge_ids, a.n, i - 1) ? advected(a, a.xy[i - 1]) : a.xy[i - 1];
+            const float2 q = movable(a.edge_ids, a.n, i + 1) ? advected(a, a.xy[i + 1]) : a.xy[i + 1];
+            out.x = __fadd_rn(s.x, __fmul_rn(a.smooth, __fsub_rn(__fmul_rn(__fadd_rn(p.x, q.x), 0.5f), s.x)));
+            out.y = __fadd_rn(s.y, __fmul_rn(a.smooth, __fsub_rn(__fmul_rn(__fadd_rn(p.y, q.y), 0.5f), s.y)));
+        }
+        a.out[i] = out;
+        if (a.counts) splat_index(out.x, out.y, a.map, &d);
     }
-    a.out[i] = out;
-    uint32_t d;
-    if (a.counts && splat_index(out.x, out.y, a.map, &d)) atomicAdd(&a.counts[d], 1u);
+    if (a.counts) {
+        // One add per texel per warp: samples climbing to the same density
+        // ridge share texels (integer counts: any order gives the same).
+        const unsigned same = __match_any_sync(0xFFFFFFFFu, d);
+        if (d != 0xFFFFFFFFu && (threadIdx.x & 31) == __ffs(same) - 1)
+            atomicAdd(&a.counts[d], static_cast<uint32_t>(__popc(same)));
+    }
 }
 
 }  // namespace

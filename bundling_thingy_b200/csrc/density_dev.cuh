@@ -16,9 +16,9 @@ constexpr int kBlurThreads = kBlurLines * kBlurSegs;
 // Three resident CTAs per SM (40 registers): the staging loads of one CTA
 // overlap the arithmetic of the others. Unbounded, the kernels took 56-70
 // registers and ran two CTAs per SM, or one (the batch's vertical pass):
-// 13.1 against 11.9 ms per iteration of 256 mixed graphs in a batch. Only the
-// batch's horizontal pass spills (20 bytes); it ran no slower than a
-// spill-free variant with taps four at a time.
+// 13.1 against 11.9 ms per iteration of 256 mixed graphs in a batch. The
+// horizontal passes spill a few bytes (4 single-graph, 20 batched); they ran
+// no slower than a spill-free variant with taps four at a time.
 constexpr int kBlurMinCtas = 3;
 
 __host__ __device__ inline int blur_padded(int R) { return (R + 7) & ~7; }
@@ -79,15 +79,20 @@ __device__ __forceinline__ void blur_h_tile(const uint32_t* __restrict__ in, flo
     const long x0 = static_cast<long>(bx) * kBlurSpan;
     const long y0 = static_cast<long>(by) * kBlurLines;
     const int width = kBlurSpan + 2 * RP;
-    for (int i = tid; i < kBlurLines * width; i += kBlurThreads) {
-        const int line = i / width, col = i - line * width;
-        const long y = y0 + line, x = x0 - RP + col;
-        float v = 0.0f;
-        if (y < H && x >= 0 && x < W) v = static_cast<float>(in[static_cast<size_t>(y) * W + x]);
-        tile[line * P + col] = v;
+    const int lane = tid & 31, seg = tid >> 5;
+    // Warp per line, lanes along it: coalesced, and no division per element.
+    for (int line = seg; line < kBlurLines; line += kBlurSegs) {
+        const long yl = y0 + line;
+        const bool row = yl < H;
+        const uint32_t* src = in + static_cast<size_t>(row ? yl : 0) * W;
+        for (int col = lane; col < width; col += 32) {
+            const long x = x0 - RP + col;
+            float v = 0.0f;
+            if (row && x >= 0 && x < W) v = static_cast<float>(src[x]);
+            tile[line * P + col] = v;
+        }
     }
     __syncthreads();
-    const int lane = tid & 31, seg = tid >> 5;
     const long y = y0 + lane;
     const long xs = x0 + seg * kBlurOut;
     if (y < H && xs < W) {
