@@ -54,17 +54,37 @@ __device__ __forceinline__ bool movable(const uint32_t* __restrict__ ids, uint32
     return i > 0 && i + 1 < n && ids[i - 1] == ids[i] && ids[i + 1] == ids[i];
 }
 
-// Every lane of the grid's warps reaches the splat (idle lanes past n too):
-// it is warp-aggregated.
-__global__ void __launch_bounds__(256) advect_kernel(AdvectArgs a) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+constexpr int kAdvectBlock = 256;
+
+// Advected position of sample j when it moves, else its position.
+__device__ __forceinline__ float2 moved_or_fixed(const AdvectArgs& a, uint32_t j) {
+    const float2 q = a.xy[j];
+    return movable(a.edge_ids, a.n, j) ? advected(a, q) : q;
+}
+
+// Each sample's advected position is evaluated once per CTA into shared
+// memory, with one halo sample on either side, and read there by its path
+// neighbours (a third of the gradient gathers and divisions of evaluating
+// both neighbours per thread). Every lane of the grid's warps reaches the
+// splat (idle lanes past n too): it is warp-aggregated.
+__global__ void __launch_bounds__(kAdvectBlock) advect_kernel(AdvectArgs a) {
+    __shared__ float2 adv[kAdvectBlock + 2];
+    const uint32_t base = blockIdx.x * kAdvectBlock;
+    const uint32_t i = base + threadIdx.x;
+    if (i < a.n) adv[threadIdx.x + 1] = moved_or_fixed(a, i);
+    // Halo: sample base - 1 (read only when sample base moves, so base > 0)
+    // and sample base + kAdvectBlock (read only when the block's last sample
+    // moves, so it exists).
+    if (threadIdx.x == 0 && base > 0) adv[0] = moved_or_fixed(a, base - 1);
+    if (threadIdx.x == 1 && base + kAdvectBlock < a.n) adv[kAdvectBlock + 1] = moved_or_fixed(a, base + kAdvectBlock);
+    __syncthreads();
     uint32_t d = 0xFFFFFFFFu;                              // no texel
     if (i < a.n) {
         float2 out = a.xy[i];
         if (movable(a.edge_ids, a.n, i)) {
-            const float2 s = advected(a, out);
-            const float2 p = movable(a.edge_ids, a.n, i - 1) ? advected(a, a.xy[i - 1]) : a.xy[i - 1];
-            const float2 q = movable(a.edge_ids, a.n, i + 1) ? advected(a, a.xy[i + 1]) : a.xy[i + 1];
+            const float2 s = adv[threadIdx.x + 1];
+            const float2 p = adv[threadIdx.x];
+            const float2 q = adv[threadIdx.x + 2];
             out.x = __fadd_rn(s.x, __fmul_rn(a.smooth, __fsub_rn(__fmul_rn(__fadd_rn(p.x, q.x), 0.5f), s.x)));
             out.y = __fadd_rn(s.y, __fmul_rn(a.smooth, __fsub_rn(__fmul_rn(__fadd_rn(p.y, q.y), 0.5f), s.y)));
         }
@@ -83,7 +103,7 @@ __global__ void __launch_bounds__(256) advect_kernel(AdvectArgs a) {
 }  // namespace
 
 void launch_advect(const AdvectArgs& a, cudaStream_t s) {
-    if (a.n) advect_kernel<<<div_up(a.n, 256), 256, 0, s>>>(a);
+    if (a.n) advect_kernel<<<div_up(a.n, static_cast<uint32_t>(kAdvectBlock)), kAdvectBlock, 0, s>>>(a);
 }
 
 }  // namespace bt
