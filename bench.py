@@ -259,7 +259,12 @@ def run_reference(args, ranks: Ranks):
     if ranks.rank != 0:
         return
     w = workload(args.edges)
-    base = cpu_sample(w, target_seconds=2.0, steps=args.steps, warmup=args.warmup)
+    # Each step is a bounded sample: about two minutes of neighbour-mean work
+    # over the whole run (at most 2 s and at least 0.25 s a step), so that the
+    # default 200 + 10 steps end within a few minutes; each step also repeats
+    # the whole-set grid index and density pass (about 0.2 s on 16 threads).
+    target = min(2.0, max(0.25, 120.0 / max(1, args.steps + args.warmup)))
+    base = cpu_sample(w, target_seconds=target, steps=args.steps, warmup=args.warmup)
     line = {
         "impl": "reference",
         "metric": METRIC, "value": base["value"], "unit": UNIT,
