@@ -9,6 +9,7 @@
 // loads this library until the process exits).
 #include <cuda_runtime.h>
 
+#include <cstdint>
 #include <mutex>
 #include <string>
 
@@ -31,7 +32,6 @@ static __device__ __align__(256) uint32_t g_noalloc_scratch[kHeadWords + kMaxTex
 
 struct DeviceSetup {
     bool done = false;
-    cudaError_t error = cudaSuccess;
     uint32_t* base = nullptr;
 };
 
@@ -40,19 +40,21 @@ DeviceSetup g_setup[kMaxDevices];
 
 // Once per device, with that device current: the device address of the static
 // array (its name in host code is only a host-side stand-in) and the blur
-// kernels' shared-memory attribute.
+// kernels' shared-memory attribute. Only a successful set-up is remembered: a
+// failed one (a transient error) is tried again by the next call.
 cudaError_t device_setup(int device, uint32_t** base) {
     std::lock_guard<std::mutex> lock(g_setup_mutex);
     DeviceSetup& s = g_setup[device];
     if (!s.done) {
         void* p = nullptr;
-        s.error = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (s.error == cudaSuccess) s.error = bt::prepare_density_kernels();
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e == cudaSuccess) e = bt::prepare_density_kernels();
+        if (e != cudaSuccess) return e;
         s.base = static_cast<uint32_t*>(p);
         s.done = true;
     }
     *base = s.base;
-    return s.error;
+    return cudaSuccess;
 }
 
 bt_status reject(bt_status code, const std::string& message) {
@@ -65,6 +67,12 @@ bt_status reject(bt_status code, const std::string& message) {
 extern "C" bt_status bt_density_noalloc(const uint32_t* counts, float* density, uint32_t width, uint32_t height,
                                         float blur_sigma, void* stream) {
     if (!counts || !density) return reject(BT_ERR_INVALID, "null device buffer");
+    // The normalisation stores four texels at a time and the horizontal pass
+    // reads whole words: a misaligned buffer would fault on the device.
+    if (reinterpret_cast<uintptr_t>(density) % 16 != 0)
+        return reject(BT_ERR_INVALID, "density output must be 16-byte aligned");
+    if (reinterpret_cast<uintptr_t>(counts) % 4 != 0)
+        return reject(BT_ERR_INVALID, "splat counts must be 4-byte aligned");
     if (width == 0 || height == 0) return reject(BT_ERR_INVALID, "density map dimensions must be nonzero");
     const unsigned long long texels = static_cast<unsigned long long>(width) * height;
     if (texels > kMaxTexels)

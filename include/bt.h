@@ -348,14 +348,17 @@ bt_status bt_server_stats_get(bt_server* server, bt_server_stats* stats);
  * renderer whose host application owns every device allocation, or a frame
  * loop that cannot take cudaMalloc's implicit device synchronisation or an
  * allocation failure mid-frame. The caller passes device pointers to
- * width*height u32 splat counts and to the width*height f32 output, and a
- * cudaStream_t as `stream` (NULL = the default stream); the call is
+ * width*height u32 splat counts (4-byte aligned) and to the width*height f32
+ * output (16-byte aligned: it is written four texels at a time); misaligned
+ * buffers are rejected with BT_ERR_INVALID before anything is launched. A
+ * cudaStream_t goes in `stream` (NULL = the default stream); the call is
  * asynchronous on that stream. It calls no cudaMalloc or cudaFree: its one
  * intermediate image lives in a file-scope static device array of
  * BT_NOALLOC_MAX_TEXELS texels, and larger maps are rejected with
  * BT_ERR_INVALID. The first call on a device performs a one-time set-up on
  * the current device (the array's device address and the kernels'
  * shared-memory attribute); make that first call before any stream capture.
+ * A set-up that fails returns BT_ERR_CUDA and is tried again by the next call.
  * Every call shares the one array per device, so calls whose work overlaps on
  * the GPU race: serialise them (one stream, or events between streams).
  * blur_sigma as bt_options.blur_sigma (0 = the fixed sigma-6 table). */

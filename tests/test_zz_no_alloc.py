@@ -55,3 +55,16 @@ def test_noalloc_rejects_maps_beyond_the_static_scratch():
     status = lib.bt_density_noalloc(ctypes.c_void_p(16), ctypes.c_void_p(16), 1025, 1024, ctypes.c_float(0.0), None)
     assert status == 3
     assert "exceeds the static scratch" in lib.bt_last_error(None).decode()
+
+
+def test_noalloc_rejects_misaligned_buffers_before_launching():
+    # The output is written four texels at a time and the counts are read as
+    # whole words: misaligned buffers are refused on the host, so nothing is
+    # launched (the addresses below are never dereferenced).
+    lib = bt.library()
+    status = lib.bt_density_noalloc(ctypes.c_void_p(256), ctypes.c_void_p(256 + 4), 64, 64, ctypes.c_float(0.0), None)
+    assert status == 3
+    assert "16-byte aligned" in lib.bt_last_error(None).decode()
+    status = lib.bt_density_noalloc(ctypes.c_void_p(256 + 2), ctypes.c_void_p(256), 64, 64, ctypes.c_float(0.0), None)
+    assert status == 3
+    assert "4-byte aligned" in lib.bt_last_error(None).decode()
