@@ -44,7 +44,7 @@ _u8p = ctypes.POINTER(ctypes.c_uint8)
 
 STATUS = {
     0: "ok", 1: "capacity overflow", 2: "count/emit mismatch", 3: "invalid input", 4: "no graph",
-    5: "memory budget", 6: "timeout", 7: "CUDA error", 8: "not configured",
+    5: "memory budget", 6: "timeout", 7: "CUDA error", 8: "not configured", 9: "cancelled",
 }
 
 
@@ -66,7 +66,8 @@ class _Options(ctypes.Structure):
         ("fine_cells", ctypes.c_uint32), ("use_graphs", ctypes.c_uint32), ("timing", ctypes.c_uint32),
         ("record_neighbors", ctypes.c_uint32), ("search_mode", ctypes.c_uint32), ("fine_cells_x", ctypes.c_uint32),
         ("palette", ctypes.c_uint32), ("msaa", ctypes.c_uint32), ("endpoint_dots", ctypes.c_uint32),
-        ("advect_step", ctypes.c_float), ("advect_smooth", ctypes.c_float),
+        ("advect_step", ctypes.c_float), ("advect_smooth", ctypes.c_float), ("wait_seconds", ctypes.c_float),
+        ("reserved_options", ctypes.c_uint32),
     ]
 
 
@@ -84,7 +85,7 @@ class _ServerOptions(ctypes.Structure):
     _fields_ = [
         ("device", ctypes.c_int32), ("max_active", ctypes.c_uint32), ("budget_bytes", ctypes.c_uint64),
         ("max_step", ctypes.c_uint32), ("solo_samples", ctypes.c_uint32), ("reserve_bytes", ctypes.c_uint64),
-        ("reserved", ctypes.c_uint32 * 4),
+        ("queue_timeout_ms", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 3),
     ]
 
 
@@ -123,6 +124,7 @@ SIGNATURES = {
     "bt_synchronize": ([_vp], ctypes.c_int32),
     "bt_iterate_timed": ([_vp, ctypes.c_uint32, _f32p], ctypes.c_int32),
     "bt_get_info": ([_vp, ctypes.POINTER(_Info)], ctypes.c_int32),
+    "bt_set_wait_seconds": ([_vp, ctypes.c_float], ctypes.c_int32),
     "bt_read_points": ([_vp, _vp, ctypes.c_size_t], ctypes.c_int32),
     "bt_read_paths": ([_vp, _vp, ctypes.c_size_t], ctypes.c_int32),
     "bt_read_segments": ([_vp, _u32p, ctypes.c_size_t], ctypes.c_int32),
@@ -165,6 +167,7 @@ SIGNATURES = {
     "bt_server_read_points": ([_vp, ctypes.c_uint64, _vp, ctypes.c_size_t], ctypes.c_int32),
     "bt_server_result": ([_vp, ctypes.c_uint64], _vp),
     "bt_server_release": ([_vp, ctypes.c_uint64], ctypes.c_int32),
+    "bt_server_cancel": ([_vp, ctypes.c_uint64], ctypes.c_int32),
     "bt_server_stats_get": ([_vp, ctypes.POINTER(_ServerStats)], ctypes.c_int32),
     "bt_graph_parse": ([ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(_vp)], ctypes.c_int32),
     "bt_graph_load": ([ctypes.c_char_p, ctypes.POINTER(_vp)], ctypes.c_int32),
@@ -246,6 +249,7 @@ class Options:
     endpoint_dots: bool = False
     advect_step: float = 0.0     # > 0: density-gradient advection (texels per iteration) instead of the mean
     advect_smooth: float = 0.0   # its Laplacian relaxation along the path, in [0, 1]
+    wait_seconds: float = 0.0    # host deadline of blocking calls (0 = 60 s, Gpu::wait, src/gpu.rs:484-490)
 
     def _struct(self) -> _Options:
         o = _Options()
@@ -270,6 +274,7 @@ class Options:
         o.endpoint_dots = int(bool(self.endpoint_dots))
         o.advect_step = float(self.advect_step)
         o.advect_smooth = float(self.advect_smooth)
+        o.wait_seconds = float(self.wait_seconds)
         return o
 
     def resample_scale(self) -> tuple[float, float]:
@@ -398,6 +403,13 @@ class Gpu:
 
     def synchronize(self) -> None:
         self._ck(library().bt_synchronize(self._h))
+
+    def set_wait_seconds(self, seconds: float) -> None:
+        """Host deadline of the blocking calls that follow (0 = 60 s, as
+        Gpu::wait, src/gpu.rs:484-490); past it they raise BtError with
+        status 6 and the queued work still finishes on the device."""
+        self._ck(library().bt_set_wait_seconds(self._h, float(seconds)))
+        self.options.wait_seconds = float(seconds)
 
     def info(self) -> Info:
         i = _Info()
@@ -673,14 +685,17 @@ class Server:
     iteration count is reached. Results stay on the device until released."""
 
     def __init__(self, device: int = 0, max_active: int = 32, budget_bytes: int = 120_000_000_000,
-                 max_step: int = 1, reserve_bytes: int = 0, solo_samples: int = 0):
+                 max_step: int = 1, reserve_bytes: int = 0, solo_samples: int = 0, queue_timeout_ms: int = 0):
         """solo_samples: requests of at least this many samples iterate on
-        their own context beside the batch (0 = 32768; 2**32 - 1 = never)."""
+        their own context beside the batch (0 = 32768; 2**32 - 1 = never).
+        queue_timeout_ms: a request not admitted this long after its arrival
+        fails with status 6 (0 = no deadline)."""
         o = _ServerOptions()
         library().bt_server_options_init(ctypes.byref(o))
         o.device, o.max_active, o.budget_bytes, o.max_step = device, max_active, budget_bytes, max_step
         o.reserve_bytes = reserve_bytes
         o.solo_samples = solo_samples
+        o.queue_timeout_ms = queue_timeout_ms
         h = _vp()
         _check(library().bt_server_create(ctypes.byref(o), ctypes.byref(h)))
         self._h = h
@@ -749,6 +764,11 @@ class Server:
     def release(self, rid: int) -> None:
         self._ck(library().bt_server_release(self._h, rid))
         self._options.pop(rid, None)
+
+    def cancel(self, rid: int) -> None:
+        """Drop a request that is still queued; it then finishes with status
+        9 (cancelled) through next(). An admitted request runs to the end."""
+        self._ck(library().bt_server_cancel(self._h, rid))
 
     def stats(self) -> dict:
         st = _ServerStats()

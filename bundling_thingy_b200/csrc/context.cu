@@ -242,13 +242,18 @@ bt_status wait(bt_ctx* c) {
     cudaError_t e = cudaEventRecord(c->done, c->stream);
     if (e != cudaSuccess) return cuda_fail(c, e, "cudaEventRecord");
     const auto start = std::chrono::steady_clock::now();
+    const double limit = c->opt.wait_seconds > 0.0f ? static_cast<double>(c->opt.wait_seconds) : kWaitSeconds;
     int spins = 0;
     while (true) {
         e = cudaEventQuery(c->done);
         if (e == cudaSuccess) break;
         if (e != cudaErrorNotReady) return cuda_fail(c, e, "device execution");
         const double waited = std::chrono::duration<double>(std::chrono::steady_clock::now() - start).count();
-        if (waited > kWaitSeconds) return fail(c, BT_ERR_TIMEOUT, "device wait exceeded 60 s");
+        if (waited > limit) {
+            char msg[96];
+            std::snprintf(msg, sizeof(msg), "device wait exceeded %g s", limit);
+            return fail(c, BT_ERR_TIMEOUT, msg);
+        }
         if (++spins < 2000) {
             std::this_thread::yield();
         } else {
@@ -405,6 +410,8 @@ bt_status validate_options(const bt_options* o, bt_ctx* c) {
         return fail(c, BT_ERR_INVALID, "choose one bundling step: the neighbour mean or density advection");
     if (o->advect_step > 0.0f && (o->width < 2 || o->height < 2))
         return fail(c, BT_ERR_INVALID, "density advection needs a map of at least 2 x 2 texels");
+    if (!(o->wait_seconds >= 0.0f) || !std::isfinite(o->wait_seconds))
+        return fail(c, BT_ERR_INVALID, "wait_seconds must be finite and >= 0");
     if (o->msaa != 0 && o->msaa != 1 && o->msaa != 2 && o->msaa != 4)
         return fail(c, BT_ERR_INVALID, "msaa must be 1, 2 or 4 samples");
     const uint64_t grid = o->neighbor_radius ? reference_grid_bytes(o->width, o->height, o->neighbor_radius) : 0;
@@ -922,6 +929,14 @@ bt_status bt_iterate_async(bt_ctx* c, uint32_t n) {
     }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(c, e, "kernel launch");
+    return BT_OK;
+}
+
+bt_status bt_set_wait_seconds(bt_ctx* c, float seconds) {
+    if (!c) return fail(nullptr, BT_ERR_INVALID, "null context");
+    if (!(seconds >= 0.0f) || !std::isfinite(seconds))
+        return fail(c, BT_ERR_INVALID, "wait_seconds must be finite and >= 0");
+    c->opt.wait_seconds = seconds;
     return BT_OK;
 }
 

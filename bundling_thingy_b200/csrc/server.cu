@@ -30,6 +30,7 @@
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
+#include <cstdio>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -57,6 +58,7 @@ struct Request {
     bt_ctx* ctx = nullptr;
     uint32_t slot = 0;
     bool delivered = false;
+    bool cancel = false;   // bt_server_cancel asked (guarded by bt_server::mu)
     bt_request_result result{};
 };
 
@@ -430,6 +432,48 @@ bool publish_ready(bt_server* s) {
     return moved;
 }
 
+// Queued requests that were cancelled, or that waited past the admission
+// deadline, finish with an error without touching the device. Returns
+// whether any did.
+bool drop_queued(bt_server* s) {
+    const double t = s->now();
+    const double limit = s->opt.queue_timeout_ms ? s->opt.queue_timeout_ms * 1e-3 : -1.0;
+    std::vector<std::pair<Request*, bt_status>> dropped;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        std::vector<Request*> waiting;   // not arrived yet: only a cancellation drops them
+        for (Request* r : s->future) {
+            if (r->cancel) {
+                dropped.emplace_back(r, BT_ERR_CANCELLED);
+            } else {
+                waiting.push_back(r);
+            }
+        }
+        s->future.swap(waiting);
+        std::deque<Request*> keep;
+        for (Request* r : s->ready) {
+            if (r->cancel) {
+                dropped.emplace_back(r, BT_ERR_CANCELLED);
+            } else if (limit >= 0.0 && t - r->arrival > limit) {
+                dropped.emplace_back(r, BT_ERR_TIMEOUT);
+            } else {
+                keep.push_back(r);
+            }
+        }
+        s->ready.swap(keep);
+    }
+    for (auto& d : dropped) {
+        if (d.second == BT_ERR_CANCELLED) {
+            publish(s, d.first, BT_ERR_CANCELLED, "cancelled before admission");
+        } else {
+            char msg[96];
+            std::snprintf(msg, sizeof(msg), "not admitted within %u ms of its arrival", s->opt.queue_timeout_ms);
+            publish(s, d.first, BT_ERR_TIMEOUT, msg);
+        }
+    }
+    return !dropped.empty();
+}
+
 void fail_running(bt_server* s, bt_status st, const std::string& msg) {
     for (Request* r : s->running) {
         bt_ctx* c = bt::batch_detach(s->batch, r->slot);
@@ -463,13 +507,14 @@ void worker_main(bt_server* s) {
                             s->future[i]);
         s->future.erase(s->future.begin(), s->future.begin() + static_cast<std::ptrdiff_t>(arrived));
 
+        const bool dropped = drop_queued(s);
         double mark_t = s->now();
         auto lap = [&](double& acc) {
             const double now = s->now();
             acc += now - mark_t;
             mark_t = now;
         };
-        bool moved = false;
+        bool moved = dropped;
         // The next batch step as soon as the previous one is done.
         if (!step_busy && !s->running.empty()) {
             // Nothing waiting to join: run the running graphs up to the first
@@ -529,8 +574,13 @@ void worker_main(bt_server* s) {
         if (s->stop) break;
         if (!s->incoming.empty() || !s->released.empty()) continue;
         if (!s->ready.empty()) {
-            // Waiting on the budget: a release wakes us.
-            s->work_cv.wait_for(lk, std::chrono::milliseconds(50));
+            // Waiting on the budget: a release wakes us (or the admission
+            // deadline of the oldest queued request).
+            double wait_s = 0.05;
+            if (s->opt.queue_timeout_ms)
+                wait_s = std::min(wait_s, std::max(1e-4, s->ready.front()->arrival + s->opt.queue_timeout_ms * 1e-3 -
+                                                             s->now()));
+            s->work_cv.wait_for(lk, std::chrono::duration<double>(wait_s));
         } else if (!s->future.empty()) {
             const double wait_s = s->future.front()->arrival - s->now();
             if (wait_s > 0) s->work_cv.wait_for(lk, std::chrono::duration<double>(std::min(wait_s, 0.05)));
@@ -707,6 +757,20 @@ bt_status bt_server_release(bt_server* s, uint64_t id) {
         --s->stats.resident_results;
     }
     s->requests.erase(it);
+    s->work_cv.notify_all();
+    return BT_OK;
+}
+
+bt_status bt_server_cancel(bt_server* s, uint64_t id) {
+    if (!s) return sfail(nullptr, BT_ERR_INVALID, "null server");
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->requests.find(id);
+    if (it == s->requests.end() || it->second->state == State::Done || it->second->state == State::Failed) {
+        s->err = "no unfinished request with this id";
+        g_server_error = s->err;
+        return BT_ERR_INVALID;
+    }
+    it->second->cancel = true;
     s->work_cv.notify_all();
     return BT_OK;
 }

@@ -17,7 +17,8 @@
  *    once. Different contexts are independent.
  *  - Host buffers are owned by the caller; the library copies in and out.
  *  - Blocking calls wait for the device with a deadline (60 s by default, as
- *    `Gpu::wait`, src/gpu.rs:484-490) and return BT_ERR_TIMEOUT past it.
+ *    `Gpu::wait`, src/gpu.rs:484-490; bt_options.wait_seconds changes it)
+ *    and return BT_ERR_TIMEOUT past it, leaving the queued work to finish.
  */
 #ifndef BT_H
 #define BT_H
@@ -29,7 +30,7 @@
 extern "C" {
 #endif
 
-#define BT_ABI_VERSION 2
+#define BT_ABI_VERSION 3
 
 typedef int32_t bt_status;
 enum {
@@ -41,7 +42,8 @@ enum {
     BT_ERR_BUDGET = 5,         /* memory budget exhausted or device allocation failed */
     BT_ERR_TIMEOUT = 6,        /* device wait deadline passed */
     BT_ERR_CUDA = 7,           /* CUDA runtime error */
-    BT_ERR_NOT_CONFIGURED = 8  /* "neighbor radius is not configured" (gpu.rs:529-532) */
+    BT_ERR_NOT_CONFIGURED = 8, /* "neighbor radius is not configured" (gpu.rs:529-532) */
+    BT_ERR_CANCELLED = 9       /* a served request cancelled before admission (bt_server_cancel) */
 };
 
 enum { BT_COLOR_BY_DENSITY = 0, BT_COLOR_BY_EDGE_ID = 1 };
@@ -78,6 +80,12 @@ typedef struct bt_options {
     float advect_step;              /* texels per iteration up the density gradient; > 0 selects the mode
                                        (neighbor_radius must then be 0; density is always accumulated) */
     float advect_smooth;            /* Laplacian relaxation towards the path neighbours, in [0, 1] */
+    /* Host deadline of every blocking call on the context, in seconds; past it
+       the call returns BT_ERR_TIMEOUT and the work stays queued on the
+       device (a later bt_synchronize can still wait for it). 0 = 60 s, the
+       reference's Gpu::wait (src/gpu.rs:484-490). */
+    float wait_seconds;
+    uint32_t reserved_options;      /* keep 0 */
 } bt_options;
 
 typedef struct bt_info {
@@ -143,6 +151,11 @@ bt_status bt_synchronize(bt_ctx* ctx);
 bt_status bt_iterate_timed(bt_ctx* ctx, uint32_t n, float* device_ms);
 
 bt_status bt_get_info(bt_ctx* ctx, bt_info* info);
+
+/* Changes the context's host deadline (bt_options.wait_seconds; 0 = 60 s) for
+ * the blocking calls that follow: the poll loop of Gpu::wait, whose limit the
+ * reference fixes at 60 s (src/gpu.rs:484-490). */
+bt_status bt_set_wait_seconds(bt_ctx* ctx, float seconds);
 
 /* 12-byte little-endian {f32 x, f32 y, u32 edge_id} records, sample order
  * (the point buffer read by distortion_snapshot, src/gpu.rs:469-482). */
@@ -278,7 +291,9 @@ typedef struct bt_server_options {
     uint64_t reserve_bytes;   /* device memory mapped into the allocator's pool at creation, so that
                                  admissions do not map memory while steps run (0 = none; at most
                                  budget_bytes) */
-    uint32_t reserved[4];
+    uint32_t queue_timeout_ms;/* a request still waiting for admission this long after its arrival
+                                 fails with BT_ERR_TIMEOUT (0 = it waits as long as it takes) */
+    uint32_t reserved[3];
 } bt_server_options;
 
 typedef struct bt_request_result {
@@ -333,6 +348,11 @@ bt_status bt_server_read_points(bt_server* server, uint64_t id, void* dst, size_
 bt_ctx* bt_server_result(bt_server* server, uint64_t id);
 /* Gives a finished or failed request's memory back to the server. */
 bt_status bt_server_release(bt_server* server, uint64_t id);
+/* Asks the server to drop a request that is still queued (not yet
+ * admitted): it then finishes with BT_ERR_CANCELLED through bt_server_next
+ * and holds no device memory. A request already admitted runs to the end and
+ * reports its own status. BT_ERR_INVALID for an unknown or finished id. */
+bt_status bt_server_cancel(bt_server* server, uint64_t id);
 bt_status bt_server_stats_get(bt_server* server, bt_server_stats* stats);
 
 /* ---- Density blur without allocation ---- */

@@ -32,10 +32,11 @@ def test_abi_version(lib):
     version = int(re.search(r"#define BT_ABI_VERSION (\d+)", header).group(1))
     assert lib.bt_abi_version() == version
     # The ctypes mirrors keep the C layouts (no padding holes in either).
-    assert ctypes.sizeof(bt._Options) == 88
+    assert ctypes.sizeof(bt._Options) == 96
     assert ctypes.sizeof(bt._Info) == 64
     assert ctypes.sizeof(bt._ServerOptions) == 48
     assert bt._ServerOptions.reserve_bytes.offset == 24
+    assert bt._Options.wait_seconds.offset == 88
 
 
 def test_options_defaults_match_reference(lib):
@@ -55,6 +56,8 @@ def test_options_defaults_match_reference(lib):
         ("max_graph_memory_bytes", 0, "budget must be nonzero"),
         ("blur_sigma", 100.0, "blur sigma"),
         ("sample_spacing", -1.0, "spacing"),
+        ("wait_seconds", -1.0, "wait_seconds"),
+        ("wait_seconds", float("inf"), "wait_seconds"),
     ],
 )
 def test_create_rejects_invalid_options_before_touching_cuda(lib, field, value, message):
