@@ -41,11 +41,11 @@ ITERATIONS_PER_JOB = 30
 MEAN_BYTES_PER_SAMPLE = 36
 
 
-def parse_args():
+def parse_args(argv=None):
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=200)
-    p.add_argument("--warmup", type=int, default=10)
+    p.add_argument("--steps", type=int, default=10, help="large workload: timed jobs (30 iterations each)")
+    p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--edges", type=int, default=100_000)
     p.add_argument("--e2e-jobs", type=int, default=3)
@@ -56,20 +56,34 @@ def parse_args():
     p.add_argument("--advect-smooth", type=float, default=0.5, help="advect workload: path relaxation weight")
     p.add_argument("--render-iterations", type=int, default=30,
                    help="render workload: mean updates before the frames are drawn")
+    p.add_argument("--steady-iterations", type=int, default=200,
+                   help="large workload: iterations of the steady-state figure past the job (0 = skip)")
+    p.add_argument("--quick", action="store_true", help="large workload only: no e2e, batched, served or CPU legs")
+    p.add_argument("--no-batched", action="store_true")
+    p.add_argument("--no-served", action="store_true")
     p.add_argument("--graphs", type=int, default=256, help="batched workload: number of graphs")
     p.add_argument("--batch-iterations", type=int, default=10)
     p.add_argument("--requests", type=int, default=1000, help="served workload: requests per rank")
     p.add_argument("--rate", type=float, default=200.0, help="served workload: mean arrivals per second")
-    p.add_argument("--capacity-requests", type=int, default=300,
-                   help="served workload: requests of the all-at-once capacity run (0 = skip)")
-    p.add_argument("--sustained-rate", type=float, default=40.0,
-                   help="served workload: a lower arrival rate both arms sustain, for latency (0 = skip)")
-    p.add_argument("--sustained-requests", type=int, default=200)
+    p.add_argument("--capacity-requests", type=int, default=200,
+                   help="served: requests of the all-at-once capacity run")
+    p.add_argument("--latency-requests", type=int, default=150,
+                   help="served: requests of each latency run at a fraction of the plain loop's capacity")
+    p.add_argument("--latency-fractions", type=float, nargs="*", default=[0.5, 0.8, 1.0])
+    p.add_argument("--solo-samples", type=int, default=0,
+                   help="served: requests of at least this many samples iterate beside the batch (0 = 32768)")
     p.add_argument("--max-active", type=int, default=32)
     p.add_argument("--max-step", type=int, default=1)
     p.add_argument("--budget-gb", type=float, default=120.0)
     p.add_argument("--reserve-gb", type=float, default=48.0, help="served workload: device memory mapped at start")
-    return p.parse_args()
+    return p.parse_args(argv)
+
+
+def pinned_buffer(nbytes: int) -> np.ndarray:
+    """Page-locked host bytes (read-backs into them run at full PCIe speed)."""
+    import torch
+
+    return torch.empty(nbytes, dtype=torch.uint8, pin_memory=True).numpy()
 
 
 # ---------------------------------------------------------------- ranks
@@ -133,6 +147,7 @@ class ClockSampler:
         self.device = device
         self.proc = None
         self.lines = []
+        self.first = threading.Event()
 
     def start(self):
         try:
@@ -147,6 +162,13 @@ class ClockSampler:
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
+            self.first.set()
+
+    def wait_first(self, timeout: float = 5.0) -> None:
+        """Block until nvidia-smi has printed its first sample, so that the
+        timed region that follows is covered from its start."""
+        if self.proc:
+            self.first.wait(timeout)
 
     def stop(self) -> dict:
         if not self.proc:
@@ -188,18 +210,13 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
-def profile_traffic():
-    """DRAM bytes (read + write) per launch of the neighbour-mean kernel from
-    the committed ncu summary (profiles/neighbor_mean_large.md), or None."""
-    path = os.path.join(ROOT, "profiles", "neighbor_mean_large.md")
-    try:
-        with open(path) as f:
-            for line in f:
-                if line.startswith("dram_bytes_per_launch:"):
-                    return int(line.split(":", 1)[1])
-    except (OSError, ValueError):
-        pass
-    return None
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of
+# the neighbour-mean kernel on the large workload, iteration 15 of a job, from
+# one ncu capture of this build:
+#   ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum --clock-control none \
+#       -k regex:neighbor_mean -s 14 -c 1 python bench.py --steps 1 --warmup 0 --quick
+# None until that capture has been taken for the current kernel.
+MEAN_TRAFFIC_BYTES = None
 
 
 def workload(edges: int):
@@ -282,64 +299,94 @@ def run_reference(args, ranks: Ranks):
 
 
 # ---------------------------------------------------------------- our arm
+# Kernels per iteration: neighbour mean, cell table (tile-sum scan + apply),
+# scatter, slot prefix (reduce + tile-sum scan + apply) on the context's
+# stream; blur H, blur V + maximum, normalise beside them.
+KERNELS_PER_ITERATION = 10
+
+
+def pinned_copy(a):
+    t = pinned_buffer(a.nbytes).view(a.dtype).reshape(a.shape)
+    t[...] = a
+    return t
+
+
 def run_ours(args, ranks: Ranks):
+    """The configured job on the large workload: upload, then 30 iterations
+    (Gpu::iterate), timed with CUDA events on the library's stream from the
+    first iteration after the upload to the last. A step is one such job; the
+    upload that resets the geometry before each step is not timed (its device
+    inputs are then resident). The steady state past the job, the stage
+    split, the end-to-end job through host buffers, the batched and served
+    workloads and the CPU baseline are reported beside it."""
     import bundling_thingy_b200 as bt
 
     w = workload(args.edges)
     device = ranks.local
+    iters = ITERATIONS_PER_JOB
     opts = bt.Options(width=w.width, height=w.height, neighbor_radius=w.radius, sample_spacing=w.spacing,
-                      blur_sigma=w.sigma, device=device, timing=True)
+                      blur_sigma=w.sigma, device=device)
     gpu = bt.Gpu(opts)
-    n = gpu.upload((w.xy, w.starts))
-    info = gpu.info()
     sampler = ClockSampler(device)
     sampler.start()
-    gpu.iterate(args.warmup)
+    sampler.wait_first()
+    n = 0
+    for _ in range(args.warmup):
+        n = gpu.upload((w.xy, w.starts))
+        gpu.iterate(iters)
+    job_ms = []
     ranks.barrier()
     gpu.synchronize()
-    ms = gpu.iterate_timed(args.steps)
+    for _ in range(args.steps):
+        n = gpu.upload((w.xy, w.starts))
+        job_ms.append(gpu.iterate_timed(iters))
     gpu.synchronize()
     ranks.barrier()
     clocks = sampler.stop()
-    stages = gpu.stage_times()
-    ms_max = ranks.max(ms)
-    points = ranks.sum(float(n) * args.steps)
-    value = points / (ms_max / 1e3)
+    info = gpu.info()
+    ms_max = ranks.max(sum(job_ms))
+    value = ranks.sum(float(n) * iters * args.steps) / (ms_max / 1e3)
 
-    mean_ms = stages.get("graph.neighbor_mean", float("nan")) / args.steps
+    # Steady state past the job: 10 more iterations, then the timed ones.
+    steady_ms = None
+    if args.steady_iterations:
+        gpu.iterate(10)
+        steady_ms = ranks.max(gpu.iterate_timed(args.steady_iterations))
+    gpu.close()
+
+    # Stage split of one job (per-stage CUDA events; the iterations run as
+    # direct launches instead of a CUDA graph): iteration 1 alone, then 2-30.
+    st = bt.Gpu(bt.Options(width=w.width, height=w.height, neighbor_radius=w.radius, sample_spacing=w.spacing,
+                           blur_sigma=w.sigma, device=device, timing=True))
+    st.upload((w.xy, w.starts))
+    st.iterate(1)
+    first = st.stage_times()
+    st.iterate(iters - 1)
+    rest = st.stage_times()
+    st.close()
+    stages = {k: first.get(k, 0.0) + rest.get(k, 0.0) for k in set(first) | set(rest)}
+    stages = dict(sorted(stages.items(), key=lambda kv: -kv[1]))
+    total_stage = sum(stages.values())
+    mean_ms = stages.get("graph.neighbor_mean", float("nan")) / iters
     peak, peak_kind = measured_peak_hbm()
     bytes_per_launch = MEAN_BYTES_PER_SAMPLE * n
     achieved = bytes_per_launch / (mean_ms / 1e3) / 1e9
-    total_stage = sum(stages.values())
-    gpu.close()
 
     # End to end through the public API with host buffers: upload the control
     # points, 30 iterations, read back the 12-byte records and the density.
-    # (--e2e-jobs 0 skips it, for short profiling runs.)
     e2e_value = job = None
     h2d = d2h = 0
     if args.e2e_jobs > 0:
-        opts_e2e = bt.Options(width=w.width, height=w.height, neighbor_radius=w.radius, sample_spacing=w.spacing,
-                              blur_sigma=w.sigma, device=device)
-        import torch
-
-        e2e_gpu = bt.Gpu(opts_e2e)
-        # Inputs and results in pinned host memory (filled outside the timed
-        # region); every job copies them in and out through the public API.
-        def pinned(a):
-            t = torch.empty(a.nbytes, dtype=torch.uint8, pin_memory=True).numpy().view(a.dtype).reshape(a.shape)
-            t[...] = a
-            return t
-
-        xy_h, starts_h = pinned(w.xy), pinned(w.starts)
-        records = torch.empty(12 * n, dtype=torch.uint8, pin_memory=True).numpy()
-        dens = torch.empty(w.width * w.height * 4, dtype=torch.uint8, pin_memory=True).numpy().view(np.float32)
+        e2e_gpu = bt.Gpu(opts)
+        xy_h, starts_h = pinned_copy(w.xy), pinned_copy(w.starts)
+        records = pinned_buffer(12 * n)
+        dens = pinned_buffer(w.width * w.height * 4).view(np.float32)
         job_times = []
         for j in range(args.e2e_jobs + 1):
             ranks.barrier()
             t0 = time.perf_counter()
             e2e_gpu.upload((xy_h, starts_h))
-            e2e_gpu.iterate(ITERATIONS_PER_JOB)
+            e2e_gpu.iterate(iters)
             e2e_gpu.read_records(records)
             e2e_gpu.read_density(dens)
             t = time.perf_counter() - t0
@@ -347,21 +394,17 @@ def run_ours(args, ranks: Ranks):
                 job_times.append(t)
         e2e_gpu.close()
         job = ranks.max(statistics.median(job_times))
-        e2e_value = ranks.sum(float(n) * ITERATIONS_PER_JOB) / job
+        e2e_value = ranks.sum(float(n) * iters) / job
         h2d = w.xy.nbytes + w.starts.nbytes
         d2h = records.nbytes + dens.nbytes
+
+    batched = batched_measure(args, ranks) if not args.no_batched else None
+    served = served_measure(args, ranks) if not args.no_served else None
 
     cpu = None
     if ranks.rank == 0 and ranks.world == 1 and not args.no_cpu_baseline:
         cpu = cpu_sample(w, target_seconds=args.cpu_seconds)
 
-    # Per iteration (profiles/launches_large.md): neighbour mean, cell table
-    # (tile-sum scan + apply), scatter, slot prefix (reduce + tile-sum scan +
-    # apply) on the context's stream; blur H, blur V + maximum, normalise
-    # (+ a tail launch when the map is not a multiple of 4 texels) beside them.
-    per_iter = 10
-    if (w.width * w.height) % 4:
-        per_iter += 1
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ranks.world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -369,25 +412,35 @@ def run_ours(args, ranks: Ranks):
         "data": "synthetic (seeded random-walk polylines; reference datasets are LFS stubs)",
         "config": {
             "workload": "large: 100k polylines (2-8 control points), 2048^2, spacing 1/1000, sigma 16 px, radius 16",
+            "step": f"one job: iterations 1-{iters} after an upload (the upload before each step is not timed)",
             "samples": n, "edges": w.edges, "grid": [w.width, w.height], "radius": w.radius, "sigma": w.sigma,
             "search_cells_per_grid_cell": {"x": info.fine_cells_x, "y": info.fine_cells,
                                            "chosen": "at upload from the graph's density"},
-            "iterations_per_job": ITERATIONS_PER_JOB,
+            "iterations_per_job": iters,
             "parallelism": f"replicas x{ranks.world}", "l2": "inputs larger than L2 (~330 MB working set per step)",
         },
+        "ms_per_iteration": ms_max / args.steps / iters,
+        "steady_state": None if steady_ms is None else {
+            "value": ranks.sum(float(n) * args.steady_iterations) / (steady_ms / 1e3), "unit": UNIT,
+            "ms_per_iteration": steady_ms / args.steady_iterations,
+            "iterations": f"{iters + 11}-{iters + 10 + args.steady_iterations} after the upload"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-                "step": f"upload + {ITERATIONS_PER_JOB} iterations + readback of records and density",
+                "step": f"upload + {iters} iterations + readback of records and density",
                 "seconds_per_job": job},
         "roofline": {
             "kernel": "neighbor_mean", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "traffic": profile_traffic(), "peak_source": peak_kind,
+            "frac": achieved / peak, "traffic": MEAN_TRAFFIC_BYTES, "peak_source": peak_kind,
             "bytes_per_launch": bytes_per_launch, "ms_per_launch": mean_ms,
-            "note": "the neighbour test is FP32-issue bound at radius 16 (~1,100 neighbours per sample)",
+            "launches": f"iterations 1-{iters} of one job",
+            "ms_iteration_1": first.get("graph.neighbor_mean"),
+            "note": "issue-bound: the exact test of each sample's boundary band at radius 16",
         },
-        "stage_ms_per_step": {k: v / args.steps for k, v in stages.items()},
+        "stage_ms_per_iteration": {k: v / iters for k, v in stages.items()},
         "stage_share": {k: v / total_stage for k, v in stages.items()} if total_stage else {},
-        "gpu_launches": per_iter * args.steps,
+        "gpu_launches": KERNELS_PER_ITERATION * iters * args.steps,
         "clocks": clocks,
+        "batched": batched,
+        "served": served,
         "cpu_baseline": cpu,
     }
     if ranks.rank == 0:
@@ -521,20 +574,33 @@ def run_advect(args, ranks: Ranks):
         print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------- sharding
+def shard(items, ranks: Ranks):
+    """The graphs one rank bundles: every world-th item from its rank (the
+    batched workload's graphs are independent; no collective)."""
+    return list(items)[ranks.rank::ranks.world]
+
+
+def served_seed(rank: int) -> int:
+    """Seed of a rank's own arrival stream (and its graphs) in the served
+    workload; rank 0 replays the workload's own seed."""
+    from bundling_thingy_b200 import synthetic
+
+    return synthetic.SEED_BASE + 4 + 7919 * rank
+
+
 # ---------------------------------------------------------------- batched
-def run_batched(args, ranks: Ranks):
+def batched_measure(args, ranks: Ranks) -> dict:
     """256 independent graphs (edges log-uniform 200-20,000, grids 256/512/1024),
     10 iterations each: one batch (persistent launches over graph x tile,
     CUDA-graph iteration) against the plain per-graph loop. Graphs are
     sharded across ranks by index (no collective)."""
-    import torch
-
     import bundling_thingy_b200 as bt
     from bundling_thingy_b200 import synthetic
 
     device = ranks.local
     iters = args.batch_iterations
-    jobs = synthetic.batched_jobs(args.graphs, iterations=iters)[ranks.rank::ranks.world]
+    jobs = shard(synthetic.batched_jobs(args.graphs, iterations=iters), ranks)
 
     def key(j):
         return (j.width, j.radius)
@@ -542,14 +608,6 @@ def run_batched(args, ranks: Ranks):
     def options(j):
         return bt.Options(width=j.width, height=j.height, neighbor_radius=j.radius, sample_spacing=j.spacing,
                           blur_sigma=j.sigma, device=device)
-
-    # Search-cell shapes are chosen per graph at upload from its density.
-    firsts = {}
-    for j in jobs:
-        firsts.setdefault(key(j), j)
-
-    def tuned_options(j):
-        return options(j)
 
     # Plain per-graph loop: one context per class, reused (Gpu::upload
     # releases the previous graph), upload + 10 x iterate + readback.
@@ -559,7 +617,7 @@ def run_batched(args, ranks: Ranks):
     def read(g):
         n = 12 * g.info().samples
         if host["buf"] is None or host["buf"].nbytes < n:
-            host["buf"] = torch.empty(max(n, 96 << 20), dtype=torch.uint8, pin_memory=True).numpy()
+            host["buf"] = pinned_buffer(max(n, 96 << 20))
         return g.read_records(host["buf"])
 
     # Warm-up of both arms to their steady state: each reused context holds
@@ -569,7 +627,7 @@ def run_batched(args, ranks: Ranks):
     for j in jobs:
         if key(j) not in largest or j.starts.size > largest[key(j)].starts.size:
             largest[key(j)] = j
-    ctxs = {k: bt.Gpu(tuned_options(j)) for k, j in firsts.items()}
+    ctxs = {k: bt.Gpu(options(j)) for k, j in largest.items()}
     for k, j in largest.items():
         ctxs[k].upload((j.xy, j.starts))
         ctxs[k].iterate(1)
@@ -593,7 +651,7 @@ def run_batched(args, ranks: Ranks):
 
     # Warm the batch kernels once (module load, first graph capture).
     warm = bt.Batch(device)
-    warm.add_many([(tuned_options(j), j.xy, j.starts) for j in jobs])
+    warm.add_many([(options(j), j.xy, j.starts) for j in jobs])
     warm.iterate(1)
     warm.close()
 
@@ -602,7 +660,7 @@ def run_batched(args, ranks: Ranks):
     ranks.barrier()
     t0 = time.perf_counter()
     batch = bt.Batch(device)
-    slots = [s for s, _ in batch.add_many([(tuned_options(j), j.xy, j.starts) for j in jobs])]
+    slots = [s for s, _ in batch.add_many([(options(j), j.xy, j.starts) for j in jobs])]
     t_add = time.perf_counter() - t0
     ti = time.perf_counter()
     batch.iterate(iters)
@@ -617,84 +675,90 @@ def run_batched(args, ranks: Ranks):
     samples = sum(batch.slot(s).info().samples for s in slots)
     # Device time of the batched iterations alone (CUDA events).
     dev_ms = batch.iterate_timed(iters)
+    shape = batch.shape() if hasattr(batch, "shape") else None
     batch.close()
 
     graphs = ranks.sum(len(jobs))
     batch_gps = graphs / ranks.max(batch_s)
     plain_gps = graphs / ranks.max(plain_s)
-    line = {
-        "metric": "batched graphs/s (256 graphs, 10 iterations each)", "value": batch_gps, "unit": "graphs/s",
-        "n_gpus": ranks.world, "higher_is_better": True, "scaling": "weak", "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "batched: 256 graphs, edges log-uniform 200-20k, grids 256/512/1024, 10 iterations",
-                   "warm": "both arms warmed first (one pass of the whole batch; plain contexts sized for the largest "
-                           "graph of each class)",
-                   "samples": int(ranks.sum(samples)), "parallelism": f"graphs sharded x{ranks.world}"},
-        "plain_graphs_per_s": plain_gps, "speedup_vs_plain": batch_gps / plain_gps,
+    return {
+        "graphs_per_s": batch_gps, "plain_graphs_per_s": plain_gps, "speedup_vs_plain": batch_gps / plain_gps,
+        "iteration_speedup_vs_plain": ranks.sum(t_iter) / ranks.sum(batch_iter_s),
         "batch_seconds": {"add_uploads": t_add, "iterations": batch_iter_s, "total": batch_s},
         "plain_seconds": {"iterations": t_iter, "total": plain_s},
-        "batched_points_iter_per_s_device": ranks.sum(samples * iters) / (ranks.max(dev_ms) / 1e3),
-        "iteration_speedup_vs_plain": t_iter / batch_iter_s,
-        "search_cells": "chosen per graph at upload from its density",
+        "device_points_iter_per_s": ranks.sum(samples * iters) / (ranks.max(dev_ms) / 1e3),
+        "graphs": int(graphs), "samples": int(ranks.sum(samples)), "iterations": iters,
+        "tuned_shape": shape,
         "bit_exact_vs_plain": exact,
+        "step": "upload + iterations + pinned readback of every graph, both arms warmed first",
+    }
+
+
+def run_batched(args, ranks: Ranks):
+    m = batched_measure(args, ranks)
+    line = {
+        "metric": f"batched graphs/s ({args.graphs} graphs, {args.batch_iterations} iterations each)",
+        "value": m["graphs_per_s"], "unit": "graphs/s", "n_gpus": ranks.world, "higher_is_better": True,
+        "scaling": "weak", "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "batched: 256 graphs, edges log-uniform 200-20k, grids 256/512/1024, 10 iterations",
+                   "parallelism": f"graphs sharded x{ranks.world}"},
+        **m,
     }
     if ranks.rank == 0:
         print(json.dumps(line), flush=True)
 
 
-def run_served(args, ranks: Ranks):
-    """Poisson-arriving requests (mean 200/s; edges log-uniform 500-50,000;
-    grids 512/1024/2048; 10 iterations each; 120 GB admission budget): the
+# ---------------------------------------------------------------- served
+class ServedBench:
+    """Poisson-arriving requests (edges log-uniform 500-50,000; grids
+    512/1024/2048; 10 iterations each; 120 GB admission budget): the
     continuous-batching server against the plain per-request loop, both
     replaying the same arrival schedule and reading every result back to
     pinned host memory. Each rank serves its own arrival stream (weak
     scaling, no collective)."""
-    import torch
-
-    import bundling_thingy_b200 as bt
-    from bundling_thingy_b200 import synthetic
-
-    device = ranks.local
-    iters = args.batch_iterations
-    arrivals, jobs = synthetic.served_jobs(args.requests, rate=args.rate, iterations=iters,
-                                           seed=synthetic.SEED_BASE + 4 + 7919 * ranks.rank)
-    n = len(jobs)
-
-    def key(j):
-        return (j.width, j.radius)
-
-    def options(j):
-        return bt.Options(width=j.width, height=j.height, neighbor_radius=j.radius, sample_spacing=j.spacing,
-                          blur_sigma=j.sigma, device=device)
-
-    firsts = {}   # (grid, radius) class -> index of its first request
-    largest = {}  # (grid, radius) class -> index of its largest request
-    for i, j in enumerate(jobs):
-        firsts.setdefault(key(j), i)
-        if key(j) not in largest or j.starts.size > jobs[largest[key(j)]].starts.size:
-            largest[key(j)] = i
-    by_size = sorted(range(n), key=lambda i: -jobs[i].starts.size)
-    warm_set = by_size[: max(len(largest), args.max_active)]
-    opts = [options(j) for j in jobs]   # search cells chosen per graph at upload
-
-    host = {"buf": None}
-
-    def pinned(nbytes):
-        if host["buf"] is None or host["buf"].nbytes < nbytes:
-            host["buf"] = torch.empty(max(nbytes, 128 << 20), dtype=torch.uint8, pin_memory=True).numpy()
-        return host["buf"]
 
     keep = 4   # results compared between the arms
 
-    def plain_run(sched):
+    def __init__(self, args, ranks: Ranks, requests: int):
+        import bundling_thingy_b200 as bt
+        from bundling_thingy_b200 import synthetic
+
+        self.bt, self.args, self.ranks = bt, args, ranks
+        self.device = ranks.local
+        self.iters = args.batch_iterations
+        self.arrivals, self.jobs = synthetic.served_jobs(requests, rate=args.rate, iterations=self.iters,
+                                                         seed=served_seed(ranks.rank))
+        self.largest = {}  # (grid, radius) class -> index of its largest request
+        for i, j in enumerate(self.jobs):
+            k = self.key(j)
+            if k not in self.largest or j.starts.size > self.jobs[self.largest[k]].starts.size:
+                self.largest[k] = i
+        by_size = sorted(range(len(self.jobs)), key=lambda i: -self.jobs[i].starts.size)
+        self.warm_set = by_size[: max(len(self.largest), args.max_active)]
+        self.opts = [bt.Options(width=j.width, height=j.height, neighbor_radius=j.radius, sample_spacing=j.spacing,
+                                blur_sigma=j.sigma, device=self.device) for j in self.jobs]
+        self.host = None
+
+    @staticmethod
+    def key(j):
+        return (j.width, j.radius)
+
+    def pinned(self, nbytes):
+        if self.host is None or self.host.nbytes < nbytes:
+            self.host = pinned_buffer(max(nbytes, 128 << 20))
+        return self.host
+
+    def plain(self, sched):
         """Plain per-request loop: one reused context per (grid, radius)
         class; upload, 10 iterations, read back, in arrival order."""
+        bt, jobs = self.bt, self.jobs
         ctxs = {}
-        for k, i in largest.items():      # each context sized for its class's largest graph
+        for k, i in self.largest.items():      # each context sized for its class's largest graph
             j = jobs[i]
-            g = bt.Gpu(opts[i])
+            g = bt.Gpu(self.opts[i])
             g.upload((j.xy, j.starts))
             g.iterate(1)
-            g.read_records(pinned(12 * g.info().samples))
+            g.read_records(self.pinned(12 * g.info().samples))
             ctxs[k] = g
         lat, kept, samples = [], {}, 0
         base = time.perf_counter() + 0.05
@@ -704,36 +768,38 @@ def run_served(args, ranks: Ranks):
             wait = target - time.perf_counter()
             if wait > 0:
                 time.sleep(wait)
-            g = ctxs[key(j)]
+            g = ctxs[self.key(j)]
             nsamp = g.upload((j.xy, j.starts))
-            g.iterate(iters)
-            rec = g.read_records(pinned(12 * nsamp))
+            g.iterate(self.iters)
+            rec = g.read_records(self.pinned(12 * nsamp))
             t_end = time.perf_counter()
             lat.append(t_end - target)
             samples += nsamp
-            if i < keep:
+            if i < self.keep:
                 kept[i] = rec.copy()
         for g in ctxs.values():
             g.close()
-        return lat, t_end - (base + sched[0]), samples, kept
+        return {"lat": lat, "span": t_end - (base + sched[0]), "samples": samples, "kept": kept}
 
-    def served_run(sched):
-        server = bt.Server(device, max_active=args.max_active, budget_bytes=int(args.budget_gb * 1e9),
-                           max_step=args.max_step, reserve_bytes=int(args.reserve_gb * 1e9))
+    def served(self, sched):
+        args, jobs = self.args, self.jobs
+        server = self.bt.Server(self.device, max_active=args.max_active, budget_bytes=int(args.budget_gb * 1e9),
+                                max_step=args.max_step, reserve_bytes=int(args.reserve_gb * 1e9),
+                                solo_samples=args.solo_samples)
         # Warm-up to the steady state: the max_active largest requests at
         # once (kernels, device memory pool, idle contexts sized for large
         # graphs, like the plain loop's reused contexts).
-        for i in warm_set:
-            server.submit(opts[i], jobs[i].xy, jobs[i].starts, 1)
-        for _ in warm_set:
+        for i in self.warm_set:
+            server.submit(self.opts[i], jobs[i].xy, jobs[i].starts, 1)
+        for _ in self.warm_set:
             r = server.next(120.0)
-            server.read_records(r.id, r.samples, pinned(12 * r.samples))
+            server.read_records(r.id, r.samples, self.pinned(12 * r.samples))
             server.release(r.id)
         t0 = time.perf_counter()
         base = server.clock() + 1.0 + 2e-3 * len(sched)   # after every submission
         ids = {}
         for i, (a, j) in enumerate(zip(sched, jobs[: len(sched)])):
-            ids[server.submit(opts[i], j.xy, j.starts, iters, arrival_s=base + a)] = i
+            ids[server.submit(self.opts[i], j.xy, j.starts, self.iters, arrival_s=base + a)] = i
         submit_s = time.perf_counter() - t0
         late = server.clock() > base
         lat, kept, samples, t_end = [], {}, 0, base
@@ -741,83 +807,100 @@ def run_served(args, ranks: Ranks):
             r = server.next(300.0)
             if r.status != 0:
                 raise RuntimeError(f"request {r.id} failed: {r.message}")
-            rec = server.read_records(r.id, r.samples, pinned(12 * r.samples))
+            rec = server.read_records(r.id, r.samples, self.pinned(12 * r.samples))
             t_end = server.clock()
             lat.append(t_end - r.arrival_s)
             samples += r.samples
-            if ids[r.id] < keep:
+            if ids[r.id] < self.keep:
                 kept[ids[r.id]] = rec.copy()
             server.release(r.id)
         stats = server.stats()
         server.close()
-        return lat, t_end - (base + sched[0]), samples, kept, stats, submit_s, late
+        return {"lat": lat, "span": t_end - (base + sched[0]), "samples": samples, "kept": kept, "stats": stats,
+                "submit_s": submit_s, "late": late}
 
-    def pct(lat):
-        return {"p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
-                "max_ms": float(np.max(lat) * 1e3)}
+    def both(self, sched):
+        self.ranks.barrier()
+        s = self.served(sched)
+        self.ranks.barrier()
+        p = self.plain(sched)
+        s["exact"] = s["samples"] == p["samples"] and all(np.array_equal(s["kept"][i], p["kept"][i])
+                                                         for i in p["kept"])
+        return s, p
 
-    ranks.barrier()
-    clocks = ClockSampler(device)
+    def rate(self, m, span):
+        return self.ranks.sum(m / self.ranks.max(span))
+
+
+def pct(lat):
+    return {"p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
+            "max_ms": float(np.max(lat) * 1e3)}
+
+
+def served_measure(args, ranks: Ranks) -> dict:
+    """Capacity of both arms (every request arrives at once), then p50/p99
+    latency of both arms at fixed fractions of the plain loop's capacity,
+    replaying the same Poisson draws on a slower or faster clock."""
+    sb = ServedBench(args, ranks, max(args.capacity_requests, args.latency_requests))
+    m = min(args.capacity_requests, len(sb.jobs))
+    cs, cp = sb.both(np.zeros(m))
+    cap_s, cap_p = sb.rate(m, cs["span"]), sb.rate(m, cp["span"])
+    out = {
+        "capacity": {"requests": m, "served_graphs_per_s": cap_s, "plain_graphs_per_s": cap_p,
+                     "speedup_vs_plain": cap_s / cap_p, "bit_exact_vs_plain": cs["exact"],
+                     "served_peak_active": cs["stats"]["peak_active"]},
+        "latency": [],
+        "config": {"iterations": sb.iters, "max_active": args.max_active, "max_step": args.max_step,
+                   "solo_samples": args.solo_samples or 32768, "budget_gb": args.budget_gb,
+                   "edges": "log-uniform 500-50k", "grids": "512/1024/2048"},
+    }
+    m = min(args.latency_requests, len(sb.jobs))
+    unit = np.asarray(sb.arrivals[:m]) * args.rate    # Poisson draws at one arrival per unit
+    for frac in args.latency_fractions:
+        rate = frac * cap_p / max(ranks.world, 1)     # per rank, against the plain loop's capacity
+        ls, lp = sb.both(unit / rate)
+        out["latency"].append({
+            "fraction_of_plain_capacity": frac, "rate_per_s": rate, "requests": m,
+            "served": pct(ls["lat"]), "plain": pct(lp["lat"]),
+            "served_graphs_per_s": sb.rate(m, ls["span"]), "plain_graphs_per_s": sb.rate(m, lp["span"]),
+            "bit_exact_vs_plain": ls["exact"]})
+    return out
+
+
+def run_served(args, ranks: Ranks):
+    """The served workload at its configured rate (Poisson 200/s) plus the
+    capacity and latency figures of served_measure."""
+    sb = ServedBench(args, ranks, args.requests)
+    clocks = ClockSampler(ranks.local)
     clocks.start()
-    s_lat, s_span, s_samples, s_kept, stats, submit_s, late = served_run(arrivals)
-    ranks.barrier()
-    p_lat, p_span, p_samples, p_kept = plain_run(arrivals)
+    clocks.wait_first()
+    s, p = sb.both(sb.arrivals)
     clock_info = clocks.stop()
-    exact = s_samples == p_samples and all(np.array_equal(s_kept[i], p_kept[i]) for i in p_kept)
-
-    capacity = None
-    if args.capacity_requests:
-        m = min(args.capacity_requests, n)
-        at_once = np.zeros(m)
-        ranks.barrier()
-        c_s = served_run(at_once)
-        ranks.barrier()
-        c_p = plain_run(at_once)
-        capacity = {"requests": m, "served_graphs_per_s": ranks.sum(m / ranks.max(c_s[1])),
-                    "plain_graphs_per_s": ranks.sum(m / ranks.max(c_p[1])),
-                    "served_peak_active": c_s[4]["peak_active"],
-                    "server": {k: c_s[4][k] for k in ("steps", "launch_s", "upload_s", "wait_s", "retire_s", "idle_s",
-                                                       "contexts_created", "create_s")}}
-        capacity["speedup_vs_plain"] = capacity["served_graphs_per_s"] / capacity["plain_graphs_per_s"]
-
-    sustained = None
-    if args.sustained_rate > 0 and args.sustained_requests > 0:
-        m = min(args.sustained_requests, n)
-        sched = np.asarray(arrivals[:m]) * (args.rate / args.sustained_rate)   # same draws, slower clock
-        ranks.barrier()
-        u_s = served_run(sched)
-        ranks.barrier()
-        u_p = plain_run(sched)
-        sustained = {"rate": args.sustained_rate, "requests": m,
-                     "served_graphs_per_s": ranks.sum(m / ranks.max(u_s[1])),
-                     "plain_graphs_per_s": ranks.sum(m / ranks.max(u_p[1])),
-                     "latency": pct(u_s[0]), "plain_latency": pct(u_p[0])}
-
-    served_gps = ranks.sum(n / ranks.max(s_span))
-    plain_gps = ranks.sum(n / ranks.max(p_span))
+    n = len(sb.jobs)
+    served_gps, plain_gps = sb.rate(n, s["span"]), sb.rate(n, p["span"])
+    stats = s["stats"]
     line = {
-        "metric": f"served graphs/s (Poisson {args.rate:g}/s, {iters} iterations each)", "value": served_gps,
+        "metric": f"served graphs/s (Poisson {args.rate:g}/s, {sb.iters} iterations each)", "value": served_gps,
         "unit": "graphs/s", "n_gpus": ranks.world, "higher_is_better": True, "scaling": "weak", "dtype": "f32",
         "data": "synthetic",
         "config": {"workload": f"served: {n} Poisson requests per rank at {args.rate:g}/s, edges log-uniform "
-                               f"500-50k, grids 512/1024/2048, {iters} iterations, "
+                               f"500-50k, grids 512/1024/2048, {sb.iters} iterations, "
                                f"{args.budget_gb:g} GB admission budget",
                    "max_active": args.max_active, "max_step": args.max_step, "reserve_gb": args.reserve_gb,
+                   "solo_samples": args.solo_samples or 32768,
                    "warm": "both arms warmed with the largest graphs first (device memory pool mapped, "
                            "contexts sized); inputs larger than L2",
-                   "search_cells": "chosen per graph at upload from its density",
                    "parallelism": f"one arrival stream per rank x{ranks.world}"},
-        "latency": pct(s_lat), "plain_latency": pct(p_lat),
+        "latency": pct(s["lat"]), "plain_latency": pct(p["lat"]),
         "plain_graphs_per_s": plain_gps, "speedup_vs_plain": served_gps / plain_gps,
-        "served_points_iter_per_s": ranks.sum(s_samples * iters / s_span),
+        "served_points_iter_per_s": ranks.sum(s["samples"] * sb.iters / s["span"]),
         "server": {k: stats[k] for k in ("peak_active", "peak_device_bytes", "budget_waits", "evictions", "steps",
                                          "launch_s", "upload_s", "wait_s", "retire_s", "idle_s", "contexts_created",
                                          "create_s")},
-        "submit_seconds": submit_s, "arrivals_late": late,
-        "capacity_all_at_once": capacity,
-        "sustained": sustained,
-        "bit_exact_vs_plain": exact,
+        "submit_seconds": s["submit_s"], "arrivals_late": s["late"],
+        "bit_exact_vs_plain": s["exact"],
         "clocks": clock_info,
+        "capacity_and_latency": served_measure(args, ranks),
     }
     if ranks.rank == 0:
         print(json.dumps(line), flush=True)
@@ -825,6 +908,8 @@ def run_served(args, ranks: Ranks):
 
 def main():
     args = parse_args()
+    if args.quick:
+        args.e2e_jobs, args.no_batched, args.no_served, args.no_cpu_baseline = 0, True, True, True
     ranks = Ranks(args.gpus)
     try:
         if args.impl == "reference":
