@@ -117,15 +117,17 @@ __global__ void __launch_bounds__(256) batch_clear_kernel(BatchArgs b) {
 // warp before it takes the next tile, so half-size tiles waste half as much
 // on graphs whose samples have very different neighbourhoods (13.35 against
 // 13.84 ms per iteration of 256 mixed graphs with 256-sample tiles).
+static_assert(kSampleTile == kMeanThreads, "one mean tile per CTA of the mean kernel's shape");
 __global__ void __launch_bounds__(kSampleTile, 10) batch_mean_kernel(BatchArgs b) {
     __shared__ uint32_t t_sh;
     __shared__ MeanArgs args;
+    __shared__ MeanShared sh;
     uint32_t t;
     while (next_tile(&b.counters[cMean], b.counts[kSamples], &t_sh, &t)) {
         const uint2 tile = b.lists[kSamples][t];
         stage_words(&args, &b.slots[tile.x].mean[b.state[tile.x].cur]);
         __syncthreads();
-        dev::mean_sample(args, tile.y + threadIdx.x);
+        dev::mean_sample(args, tile.y + threadIdx.x, sh.ranges[threadIdx.x >> 5]);
     }
 }
 
