@@ -296,12 +296,26 @@ void drop_graphs(bt_ctx* c) {
 bt_status enqueue_density(bt_ctx* c, uint32_t pass, cudaStream_t stream) {
     bt::Taps taps;
     if (!blur_taps(sigma_for_pass(c->opt, pass), &taps)) return fail(c, BT_ERR_INVALID, "invalid blur sigma");
+    // TMA-staged passes (blur_tma.cu) when the map's rows are whole 16-byte
+    // units; element-staged ones (density.cu) otherwise. Same results.
+    const bool tma = bt::blur_tma_eligible(c->counts.p, c->himg.p, c->map.w, c->map.h) &&
+                     bt::blur_tma_eligible(c->himg.p, c->vimg.p, c->map.w, c->map.h);
     stage_begin(c, "density.blur_horizontal", stream);
-    bt::launch_blur_horizontal(c->counts.as<uint32_t>(), c->himg.as<float>(), c->map.w, c->map.h, taps, stream);
+    if (tma) {
+        BT_CUDA(c, bt::launch_blur_horizontal_tma(c->counts.as<uint32_t>(), c->himg.as<float>(), c->map.w, c->map.h,
+                                                   taps, c->status.as<uint32_t>(), stream));
+    } else {
+        bt::launch_blur_horizontal(c->counts.as<uint32_t>(), c->himg.as<float>(), c->map.w, c->map.h, taps, stream);
+    }
     stage_end(c, stream);
     stage_begin(c, "density.blur_vertical_and_maximum", stream);
-    bt::launch_blur_vertical(c->himg.as<float>(), c->vimg.as<float>(), c->map.w, c->map.h, taps,
-                             c->peak.as<uint32_t>(), stream);
+    if (tma) {
+        BT_CUDA(c, bt::launch_blur_vertical_tma(c->himg.as<float>(), c->vimg.as<float>(), c->map.w, c->map.h, taps,
+                                                 c->peak.as<uint32_t>(), c->status.as<uint32_t>(), stream));
+    } else {
+        bt::launch_blur_vertical(c->himg.as<float>(), c->vimg.as<float>(), c->map.w, c->map.h, taps,
+                                 c->peak.as<uint32_t>(), stream);
+    }
     stage_end(c, stream);
     stage_begin(c, "density.normalize", stream);
     bt::launch_normalize(c->vimg.as<float>(), c->peak.as<uint32_t>(), c->norm.as<float>(), c->texels, stream);
@@ -844,6 +858,7 @@ bt_status bt::upload_adapt(bt_ctx* c) {
 bt_status bt::upload_check(bt_ctx* c, uint32_t* out_samples) {
     if (c->h_status[0] & 2u) return fail(c, BT_ERR_MISMATCH, "GPU resampling count and write passes disagree");
     if (c->h_status[0] & 8u) return fail(c, BT_ERR_CUDA, "inconsistent neighbour-grid binning");
+    if (c->h_status[0] & 16u) return fail(c, BT_ERR_TIMEOUT, "a density tile copy did not complete on the device");
     c->uploaded = true;
     *out_samples = c->samples;
     return BT_OK;
@@ -979,6 +994,7 @@ bt_status check_iteration_status(bt_ctx* c) {
         c->uploaded = false;
         return fail(c, BT_ERR_CUDA, "inconsistent neighbour-grid binning");
     }
+    if (c->h_status[0] & 16u) return fail(c, BT_ERR_TIMEOUT, "a density tile copy did not complete on the device");
     return BT_OK;
 }
 }  // namespace

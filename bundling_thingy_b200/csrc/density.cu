@@ -70,8 +70,10 @@ cudaError_t prepare_density_kernels() {
     cudaError_t e = cudaFuncSetAttribute(reinterpret_cast<const void*>(blur_h_kernel),
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(reinterpret_cast<const void*>(blur_v_kernel),
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    e = cudaFuncSetAttribute(reinterpret_cast<const void*>(blur_v_kernel),
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e != cudaSuccess) return e;
+    return prepare_blur_tma_kernels();
 }
 
 void launch_blur_horizontal(const uint32_t* counts, float* out, uint32_t w, uint32_t h, const Taps& taps,
