@@ -156,6 +156,10 @@ SIGNATURES = {
     "bt_batch_slot_count": ([_vp, _u32p, _u32p], ctypes.c_int32),
     "bt_batch_set_solo_samples": ([_vp, ctypes.c_uint32], ctypes.c_int32),
     "bt_batch_slot": ([_vp, ctypes.c_uint32], _vp),
+    "bt_batch_set_shape": ([_vp, ctypes.c_uint32, ctypes.c_uint32], ctypes.c_int32),
+    "bt_batch_get_shape": ([_vp, _u32p, _u32p], ctypes.c_int32),
+    "bt_batch_autotune": ([ctypes.c_int32, ctypes.c_uint32, ctypes.POINTER(_Options), ctypes.POINTER(_f32p), _u32p,
+                           ctypes.POINTER(_u32p), _u32p, ctypes.c_uint32, _u32p, _u32p, _f32p], ctypes.c_int32),
     "bt_server_options_init": ([ctypes.POINTER(_ServerOptions)], None),
     "bt_server_create": ([ctypes.POINTER(_ServerOptions), ctypes.POINTER(_vp)], ctypes.c_int32),
     "bt_server_destroy": ([_vp], None),
@@ -576,6 +580,38 @@ class Batch:
         self._options: dict[int, Options] = {}
         if solo_samples:
             self.set_solo_samples(solo_samples)
+
+    def set_shape(self, mean_tile: int = 128, mean_ctas_per_sm: int = 0) -> None:
+        """bt_batch_set_shape: samples per mean tile (64, 128, 256) and resident
+        mean CTAs per SM (0 = as many as fit); results do not depend on it."""
+        self._ck(library().bt_batch_set_shape(self._h, mean_tile, mean_ctas_per_sm))
+
+    def shape(self) -> dict:
+        t = np.zeros(1, np.uint32)
+        c = np.zeros(1, np.uint32)
+        self._ck(library().bt_batch_get_shape(self._h, _p(t, _u32p), _p(c, _u32p)))
+        return {"mean_tile": int(t[0]), "mean_ctas_per_sm": int(c[0])}
+
+    @staticmethod
+    def autotune(jobs, iterations: int = 3, device: int = 0) -> tuple[dict, float]:
+        """bt_batch_autotune over (options, xy, starts) triples: the fastest
+        batch shape for these graphs and its time for `iterations` iterations."""
+        jobs = list(jobs)
+        n = len(jobs)
+        opts = (_Options * n)(*[o._struct() for o, _, _ in jobs])
+        xys = [np.ascontiguousarray(xy, np.float32) for _, xy, _ in jobs]
+        sts = [np.ascontiguousarray(st, np.uint32) for _, _, st in jobs]
+        xy_ptrs = (_f32p * n)(*[_p(a, _f32p) for a in xys])
+        st_ptrs = (_u32p * n)(*[_p(a, _u32p) for a in sts])
+        n_points = np.array([a.size // 2 for a in xys], np.uint32)
+        n_starts = np.array([a.size for a in sts], np.uint32)
+        t = np.zeros(1, np.uint32)
+        c = np.zeros(1, np.uint32)
+        ms = np.zeros(1, np.float32)
+        _check(library().bt_batch_autotune(device, n, opts, xy_ptrs, _p(n_points, _u32p), st_ptrs,
+                                           _p(n_starts, _u32p), iterations, _p(t, _u32p), _p(c, _u32p),
+                                           _p(ms, _f32p)))
+        return {"mean_tile": int(t[0]), "mean_ctas_per_sm": int(c[0])}, float(ms[0])
 
     def set_solo_samples(self, samples: int) -> None:
         """bt_batch_set_solo_samples: the slot size from which slots iterate on

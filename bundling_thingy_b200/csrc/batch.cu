@@ -67,7 +67,7 @@ struct SlotState {
     uint32_t cur, pass, iterations, pad;
 };
 
-enum List : int { kSamples, kCells, kSlots, kPrefix, kBlurH, kBlurV, kTexels, kLists };
+enum List : int { kSamples, kMeanTiles, kCells, kSlots, kPrefix, kBlurH, kBlurV, kTexels, kLists };
 enum Counter : int {
     cClear, cMean, cCellScan, cCellApply, cScatter, cPrefixReduce, cPrefixScan, cPrefixApply, cBlurH, cBlurV,
     cNormalize, cCounters
@@ -112,23 +112,34 @@ __global__ void __launch_bounds__(256) batch_clear_kernel(BatchArgs b) {
     }
 }
 
-// Forty resident warps per SM as ten CTAs of 128 (the staged descriptor costs
-// registers that a 48th warp would spill). Each CTA waits for its slowest
-// warp before it takes the next tile, so half-size tiles waste half as much
-// on graphs whose samples have very different neighbourhoods (13.35 against
-// 13.84 ms per iteration of 256 mixed graphs with 256-sample tiles).
-static_assert(kSampleTile == kMeanThreads, "one mean tile per CTA of the mean kernel's shape");
-__global__ void __launch_bounds__(kSampleTile, 10) batch_mean_kernel(BatchArgs b) {
+// One mean tile per CTA of kThreads samples, at most 1,024 resident threads
+// per SM (thirty-two warps: with the staged descriptor and the range walk,
+// forty would spill). A CTA waits for its slowest warp before it takes the next
+// tile, so smaller tiles waste less on graphs whose samples have very
+// different neighbourhoods, and larger ones stage fewer descriptors: the
+// tile size and the resident CTAs per SM are chosen per batch
+// (bt_batch_set_shape, bt_batch_autotune).
+template <int kThreads>
+__global__ void __launch_bounds__(kThreads, 1024 / kThreads) batch_mean_kernel(BatchArgs b) {
     __shared__ uint32_t t_sh;
     __shared__ MeanArgs args;
-    __shared__ MeanShared sh;
+    __shared__ uint2 ranges[kThreads / 32][kMeanRanges][32];
     uint32_t t;
-    while (next_tile(&b.counters[cMean], b.counts[kSamples], &t_sh, &t)) {
-        const uint2 tile = b.lists[kSamples][t];
+    while (next_tile(&b.counters[cMean], b.counts[kMeanTiles], &t_sh, &t)) {
+        const uint2 tile = b.lists[kMeanTiles][t];
         stage_words(&args, &b.slots[tile.x].mean[b.state[tile.x].cur]);
         __syncthreads();
-        dev::mean_sample(args, tile.y + threadIdx.x, sh.ranges[threadIdx.x >> 5]);
+        dev::mean_sample(args, tile.y + threadIdx.x, ranges[threadIdx.x >> 5]);
     }
+}
+
+template <int kThreads>
+const void* mean_kernel_fn() {
+    return reinterpret_cast<const void*>(batch_mean_kernel<kThreads>);
+}
+
+const void* mean_kernel_for(uint32_t tile) {
+    return tile == 64 ? mean_kernel_fn<64>() : tile == 256 ? mean_kernel_fn<256>() : mean_kernel_fn<128>();
 }
 
 // Cell table: the population sums per tile (accumulated by the mean kernel)
@@ -314,6 +325,8 @@ struct bt_batch {
     uint32_t* h_status = nullptr;
     uint32_t max_pass = 0;     // highest density pass the taps tables cover
     uint32_t solo_samples = bt::kNeverSolo;
+    uint32_t mean_tile = 128;        // samples per mean tile (= its CTA size): 64, 128 or 256
+    uint32_t mean_ctas_per_sm = 0;   // resident mean CTAs per SM (0 = as many as fit)
 };
 
 namespace bt {
@@ -446,7 +459,11 @@ void enqueue_batch_iteration(bt_batch* b) {
     const BatchArgs a = batch_args(b);
     cudaMemsetAsync(b->counters.p, 0, sizeof(uint32_t) * cCounters, b->stream);
     batch_clear_kernel<<<b->grid_blocks[cClear], 256, 0, b->stream>>>(a);
-    batch_mean_kernel<<<b->grid_blocks[cMean], kSampleTile, 0, b->stream>>>(a);
+    switch (b->mean_tile) {
+        case 64: batch_mean_kernel<64><<<b->grid_blocks[cMean], 64, 0, b->stream>>>(a); break;
+        case 256: batch_mean_kernel<256><<<b->grid_blocks[cMean], 256, 0, b->stream>>>(a); break;
+        default: batch_mean_kernel<128><<<b->grid_blocks[cMean], 128, 0, b->stream>>>(a); break;
+    }
     batch_cell_scan_kernel<<<b->grid_blocks[cCellScan], kScanBlock, 0, b->stream>>>(a);
     batch_cell_apply_kernel<<<b->grid_blocks[cCellApply], kScanBlock, 0, b->stream>>>(a);
     batch_scatter_kernel<<<b->grid_blocks[cScatter], kSampleTile, 0, b->stream>>>(a);
@@ -499,6 +516,8 @@ bt_status rebuild(bt_batch* b) {
         const uint32_t slot = static_cast<uint32_t>(i);
         for (uint32_t t = 0; t < (c->samples + kSampleTile - 1) / kSampleTile; ++t)
             lists[kSamples].push_back(make_uint2(slot, t * kSampleTile));
+        for (uint32_t t = 0; t < (c->samples + b->mean_tile - 1) / b->mean_tile; ++t)
+            lists[kMeanTiles].push_back(make_uint2(slot, t * b->mean_tile));
         for (uint32_t t = 0; t < cell_tiles; ++t) lists[kCells].push_back(make_uint2(slot, t));
         for (uint32_t t = 0; t < prefix_tiles; ++t) lists[kPrefix].push_back(make_uint2(slot, t));
         lists[kSlots].push_back(make_uint2(slot, 0u));
@@ -528,6 +547,16 @@ bt_status rebuild(bt_batch* b) {
     }
     BB_CUDA(b, cudaMemcpyAsync(b->counts.p, counts, sizeof(counts), cudaMemcpyHostToDevice, b->stream));
     if (bt_status st = bwait(b)) return st;   // the host vectors go out of scope
+    {
+        // The mean's persistent grid for the batch's shape.
+        int per_sm = 0;
+        cudaError_t oe = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mean_kernel_for(b->mean_tile),
+                                                                       static_cast<int>(b->mean_tile), 0);
+        if (oe != cudaSuccess) return bcuda(b, oe, "occupancy");
+        per_sm = std::max(1, per_sm);
+        if (b->mean_ctas_per_sm) per_sm = std::min(per_sm, static_cast<int>(b->mean_ctas_per_sm));
+        b->grid_blocks[cMean] = per_sm * b->sms;
+    }
     if (b->graph) {
         cudaGraphExecDestroy(b->graph);
         b->graph = nullptr;
@@ -645,7 +674,6 @@ bt_status bt_batch_create(int32_t device, bt_batch** out) {
         size_t smem;
     } ks[] = {
         {cClear, reinterpret_cast<const void*>(batch_clear_kernel), 256, 0},
-        {cMean, reinterpret_cast<const void*>(batch_mean_kernel), kSampleTile, 0},
         {cCellScan, reinterpret_cast<const void*>(batch_cell_scan_kernel), kScanBlock, 0},
         {cCellApply, reinterpret_cast<const void*>(batch_cell_apply_kernel), kScanBlock, 0},
         {cScatter, reinterpret_cast<const void*>(batch_scatter_kernel), kSampleTile, 0},
@@ -858,6 +886,65 @@ bt_status bt_batch_set_solo_samples(bt_batch* b, uint32_t samples) {
     for (Slot& s : b->slots)
         if (s.active) s.solo = s.ctx->samples >= b->solo_samples;
     b->dirty = true;
+    return BT_OK;
+}
+
+bt_status bt_batch_set_shape(bt_batch* b, uint32_t mean_tile, uint32_t mean_ctas_per_sm) {
+    if (!b) return bfail(nullptr, BT_ERR_INVALID, "null batch");
+    if (mean_tile != 64 && mean_tile != 128 && mean_tile != 256)
+        return bfail(b, BT_ERR_INVALID, "mean_tile must be 64, 128 or 256 samples");
+    if (mean_ctas_per_sm > 1024 / mean_tile)
+        return bfail(b, BT_ERR_INVALID, "mean_ctas_per_sm above the 1,024 resident threads of the mean kernel");
+    cudaSetDevice(b->device);
+    if (bt_status s = bwait(b)) return s;   // no step in flight while the work lists change
+    b->mean_tile = mean_tile;
+    b->mean_ctas_per_sm = mean_ctas_per_sm;
+    b->dirty = true;
+    return BT_OK;
+}
+
+bt_status bt_batch_get_shape(bt_batch* b, uint32_t* mean_tile, uint32_t* mean_ctas_per_sm) {
+    if (!b || !mean_tile || !mean_ctas_per_sm) return bfail(b, BT_ERR_INVALID, "null argument");
+    *mean_tile = b->mean_tile;
+    *mean_ctas_per_sm = b->mean_ctas_per_sm;
+    return BT_OK;
+}
+
+bt_status bt_batch_autotune(int32_t device, uint32_t count, const bt_options* options, const float* const* xy,
+                            const uint32_t* n_points, const uint32_t* const* starts, const uint32_t* n_starts,
+                            uint32_t iterations, uint32_t* mean_tile, uint32_t* mean_ctas_per_sm, float* best_ms) {
+    if (!mean_tile || !mean_ctas_per_sm || count == 0 || iterations == 0)
+        return bfail(nullptr, BT_ERR_INVALID, "null argument, no graph or no iteration");
+    // Each candidate on a fresh scratch batch of the same graphs, so that
+    // every candidate times the same iterations (the work per iteration
+    // changes as the graphs bundle); the caller's batch is not touched.
+    struct Cand {
+        uint32_t tile, ctas;
+    };
+    const Cand cands[] = {{64, 0}, {64, 12}, {128, 0}, {128, 6}, {256, 0}, {256, 3}};
+    std::vector<uint32_t> slots(count), samples(count);
+    float best = -1.0f;
+    for (const Cand& k : cands) {
+        bt_batch* b = nullptr;
+        if (bt_status s = bt_batch_create(device, &b)) return s;
+        bt_status s = bt_batch_add_many(b, count, options, xy, n_points, starts, n_starts, slots.data(),
+                                        samples.data());
+        if (!s) s = bt_batch_set_shape(b, k.tile, k.ctas);
+        float ms = 0.0f;
+        if (!s) s = bt_batch_iterate_timed(b, iterations, &ms);
+        if (s) {
+            const std::string msg = b->err;
+            bt_batch_destroy(b);
+            return bfail(nullptr, s, msg);
+        }
+        bt_batch_destroy(b);
+        if (best < 0.0f || ms < best) {
+            best = ms;
+            *mean_tile = k.tile;
+            *mean_ctas_per_sm = k.ctas;
+        }
+    }
+    if (best_ms) *best_ms = best;
     return BT_OK;
 }
 

@@ -258,6 +258,22 @@ bt_status bt_batch_slot_count(bt_batch* batch, uint32_t* active, uint32_t* capac
  * maps run faster in the step. Applies to every slot from the next
  * iteration; results are the same either way. */
 bt_status bt_batch_set_solo_samples(bt_batch* batch, uint32_t samples);
+/* Work shape of the batch's neighbour-mean step (the reference's counterpart
+ * knob is the compute workgroup size of its kernels, src/neighbor_mean.rs:4,
+ * src/resampling.rs:19): samples per mean tile, which is also the CTA size
+ * (64, 128 or 256; default 128), and resident mean CTAs per SM (0 = as many
+ * as fit, the default). Results do not depend on it; from the next step. */
+bt_status bt_batch_set_shape(bt_batch* batch, uint32_t mean_tile, uint32_t mean_ctas_per_sm);
+bt_status bt_batch_get_shape(bt_batch* batch, uint32_t* mean_tile, uint32_t* mean_ctas_per_sm);
+/* Autotuner of the batch shape (beyond the reference): uploads the graphs
+ * (arguments as bt_batch_add_many) into a scratch batch for each candidate
+ * shape, times `iterations` iterations after the upload (CUDA events) and
+ * returns the fastest shape (its time to *best_ms when not NULL). The
+ * caller's own batches are not touched; pass the result to
+ * bt_batch_set_shape. */
+bt_status bt_batch_autotune(int32_t device, uint32_t count, const bt_options* options, const float* const* xy,
+                            const uint32_t* n_points, const uint32_t* const* starts, const uint32_t* n_starts,
+                            uint32_t iterations, uint32_t* mean_tile, uint32_t* mean_ctas_per_sm, float* best_ms);
 /* The context of a slot, for the bt_read_* and bt_get_info calls; owned by
  * the batch (do not destroy or iterate it). Waits for the batch's work. */
 bt_ctx* bt_batch_slot(bt_batch* batch, uint32_t slot);

@@ -179,3 +179,39 @@ def test_slots_change_lanes_between_iterations():
     batch.iterate(1)
     for (w, o), slot in zip(jobs, slots):
         check_slot(batch, slot, standalone(w, o, 5))
+
+
+@pytest.mark.parametrize("mean_tile,ctas", [(64, 0), (128, 6), (256, 0), (256, 3)])
+def test_batch_shapes_do_not_change_results(mean_tile, ctas):
+    # The mean tile (= CTA size) and the resident CTAs per SM change only how
+    # the work is cut and scheduled, never a slot's results.
+    jobs = mixed_jobs()
+    batch = bt.Batch()
+    batch.set_shape(mean_tile, ctas)
+    assert batch.shape() == {"mean_tile": mean_tile, "mean_ctas_per_sm": ctas}
+    slots = [batch.add(o, w.xy, w.starts)[0] for w, o in jobs]
+    batch.iterate(2)
+    for (w, o), slot in zip(jobs, slots):
+        check_slot(batch, slot, standalone(w, o, 2))
+    # A change of shape between steps keeps the results too.
+    batch.set_shape(128, 0)
+    batch.iterate(1)
+    for (w, o), slot in zip(jobs, slots):
+        check_slot(batch, slot, standalone(w, o, 3))
+    batch.close()
+
+
+def test_autotuned_batch_matches_standalone_runs():
+    jobs = mixed_jobs()
+    shape, ms = bt.Batch.autotune([(o, w.xy, w.starts) for w, o in jobs], iterations=2)
+    assert ms > 0 and shape["mean_tile"] in (64, 128, 256)
+    batch = bt.Batch()
+    batch.set_shape(**shape)
+    slots = [batch.add(o, w.xy, w.starts)[0] for w, o in jobs]
+    batch.iterate(3)
+    for (w, o), slot in zip(jobs, slots):
+        check_slot(batch, slot, standalone(w, o, 3))
+    batch.close()
+    with pytest.raises(bt.BtError) as e:
+        bt.Batch().set_shape(96, 0)
+    assert e.value.status == 3
