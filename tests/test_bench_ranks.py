@@ -111,6 +111,13 @@ class _FakeBatch:
     def __init__(self, device=0):
         self.slots = []
 
+    @staticmethod
+    def autotune(jobs, iterations=3, device=0):
+        return {"mean_tile": 128, "mean_ctas_per_sm": 0}, 1.0
+
+    def set_shape(self, mean_tile=128, mean_ctas_per_sm=0):
+        pass
+
     def add_many(self, items):
         out = []
         for o, xy, starts in items:
