@@ -112,24 +112,23 @@ __global__ void __launch_bounds__(256) batch_clear_kernel(BatchArgs b) {
     }
 }
 
-// One mean tile per CTA of kThreads samples, at most 1,024 resident threads
-// per SM (thirty-two warps: with the staged descriptor and the range walk,
-// forty would spill). A CTA waits for its slowest warp before it takes the next
+// One mean tile per CTA of kThreads samples, at most 1,280 resident threads
+// per SM (forty warps; the staged descriptor costs registers that more
+// would spill). A CTA waits for its slowest warp before it takes the next
 // tile, so smaller tiles waste less on graphs whose samples have very
 // different neighbourhoods, and larger ones stage fewer descriptors: the
 // tile size and the resident CTAs per SM are chosen per batch
 // (bt_batch_set_shape, bt_batch_autotune).
 template <int kThreads>
-__global__ void __launch_bounds__(kThreads, 1024 / kThreads) batch_mean_kernel(BatchArgs b) {
+__global__ void __launch_bounds__(kThreads, 1280 / kThreads) batch_mean_kernel(BatchArgs b) {
     __shared__ uint32_t t_sh;
     __shared__ MeanArgs args;
-    __shared__ uint2 ranges[kThreads / 32][kMeanRanges][32];
     uint32_t t;
     while (next_tile(&b.counters[cMean], b.counts[kMeanTiles], &t_sh, &t)) {
         const uint2 tile = b.lists[kMeanTiles][t];
         stage_words(&args, &b.slots[tile.x].mean[b.state[tile.x].cur]);
         __syncthreads();
-        dev::mean_sample(args, tile.y + threadIdx.x, ranges[threadIdx.x >> 5]);
+        dev::mean_sample(args, tile.y + threadIdx.x);
     }
 }
 
@@ -893,8 +892,8 @@ bt_status bt_batch_set_shape(bt_batch* b, uint32_t mean_tile, uint32_t mean_ctas
     if (!b) return bfail(nullptr, BT_ERR_INVALID, "null batch");
     if (mean_tile != 64 && mean_tile != 128 && mean_tile != 256)
         return bfail(b, BT_ERR_INVALID, "mean_tile must be 64, 128 or 256 samples");
-    if (mean_ctas_per_sm > 1024 / mean_tile)
-        return bfail(b, BT_ERR_INVALID, "mean_ctas_per_sm above the 1,024 resident threads of the mean kernel");
+    if (mean_ctas_per_sm > 1280 / mean_tile)
+        return bfail(b, BT_ERR_INVALID, "mean_ctas_per_sm above the 1,280 resident threads of the mean kernel");
     cudaSetDevice(b->device);
     if (bt_status s = bwait(b)) return s;   // no step in flight while the work lists change
     b->mean_tile = mean_tile;
@@ -921,7 +920,7 @@ bt_status bt_batch_autotune(int32_t device, uint32_t count, const bt_options* op
     struct Cand {
         uint32_t tile, ctas;
     };
-    const Cand cands[] = {{64, 0}, {64, 12}, {128, 0}, {128, 6}, {256, 0}, {256, 3}};
+    const Cand cands[] = {{64, 0}, {64, 14}, {128, 0}, {128, 7}, {256, 0}, {256, 3}};
     std::vector<uint32_t> slots(count), samples(count);
     float best = -1.0f;
     for (const Cand& k : cands) {

@@ -74,14 +74,6 @@ struct Grid {
     float r2;            // f32(radius) * f32(radius)
     float reachx, reachy;// f32(radius) + f32(size) * 2.4e-7 (neighbor_mean.wgsl:180-181)
     float margin;        // conservative slack of the search-cell bounds, texels
-    // Exact f32 accumulation of neighbour displacements (grid_dev.cuh): a
-    // sample with |p.x| >= fast_x and |p.y| >= fast_y has every accepted
-    // neighbour q and itself on one 2^(k-23) grid with k >= -7, |q - p| <
-    // 2^(k+1), so q - p is exact in f32 and equals (Q(q) - Q(p)) / 2^30.
-    // split = 1.5 * 2^(k+12) per axis cuts such a difference into a part on
-    // the 2^(k-11) grid and an exact remainder (infinite thresholds: never).
-    float fast_x, fast_y;
-    float split_x, split_y;
 };
 
 // texel_position (spatial_grid.wgsl:59-61), one axis.

@@ -183,26 +183,6 @@ uint64_t reference_grid_bytes(uint32_t w, uint32_t h, uint32_t r) {
     return cells * 8 + 8 + cells * 24 + 52;
 }
 
-// Bounds of the exact f32 accumulation along one axis (common.cuh, Grid):
-// an accepted neighbour passes dot((q-p)*ts, (q-p)*ts) <= r*r, so |q - p| <=
-// r/ts (widened here far beyond the f32 rounding of that test). With dmax <
-// 2^(k+1) and k >= -7, a sample at |p| >= 2^k + dmax has every accepted q at
-// |q| >= 2^k: both are multiples of 2^(k-23) (so of 2^-30, where
-// Q(v) = v * 2^30 exactly) and their difference, a multiple of 2^(k-23)
-// below 2^(k+1), is exact in f32.
-void fast_accumulation_bounds(float rf, float ts, float* threshold, float* split) {
-    const double dmax = static_cast<double>(rf) / static_cast<double>(ts) * 1.0001;
-    int k = -7;
-    while (std::ldexp(1.0, k + 1) <= dmax) ++k;
-    if (!(ts > 0.0f) || k > 0) {   // positions lie in [-1, 1]: never
-        *threshold = INFINITY;
-        *split = 0.0f;
-        return;
-    }
-    *threshold = std::nextafter(static_cast<float>(std::ldexp(1.0, k) + dmax), INFINITY);
-    *split = static_cast<float>(1.5 * std::ldexp(1.0, k + 12));
-}
-
 void set_search_shape(bt::Grid& g, uint32_t ky, uint32_t kx) {
     g.ky = ky;
     g.kx = kx;
@@ -630,8 +610,6 @@ bt_status bt::create_context(const bt_options* options, bt::MemAccount* account,
         g.reachx = g.rf + static_cast<float>(W) * 0.00000024f;
         g.reachy = g.rf + static_cast<float>(H) * 0.00000024f;
         g.margin = 1e-3f + 1e-6f * static_cast<float>(std::max(W, H)) + 1e-5f * g.rf;
-        fast_accumulation_bounds(g.rf, g.tsx, &g.fast_x, &g.split_x);
-        fast_accumulation_bounds(g.rf, g.tsy, &g.fast_y, &g.split_y);
         c->cells = static_cast<size_t>(g.fw) * g.fh;
         if (c->cells > 0x7FFFFFFFull) return bail(fail(c, BT_ERR_INVALID, "neighbour search grid too large"));
         c->grid_bytes_ref = reference_grid_bytes(W, H, r);
@@ -761,9 +739,7 @@ bt_status bt::upload_finish(bt_ctx* c) {
     if (bt_status s = ensure(c, c->tmp_cell, 4ull * N)) return s;
     if (c->has_grid) {
         for (int b = 0; b < 2; ++b) {
-            // Padded: the mean kernel loads whole groups of candidates and
-            // masks the ones past a range's end.
-            if (bt_status s = ensure(c, c->sorted_rec[b], 8ull * (N + bt::kRecordPad))) return s;
+            if (bt_status s = ensure(c, c->sorted_rec[b], 8ull * N)) return s;
             if (bt_status s = ensure(c, c->sorted_tag[b], 4ull * N)) return s;
         }
         if (bt_status s = ensure(c, c->slot_prefix, 16ull * (N + 1ull))) return s;

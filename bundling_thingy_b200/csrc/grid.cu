@@ -45,9 +45,8 @@ namespace {
 // the large workload; four: 0.92). Ten CTAs of 128 rather than five of 256:
 // samples of very different neighbourhood sizes share an SM at a finer
 // grain, which trims the tail (0.845 against 0.863 ms; 64 threads: 0.849).
-__global__ void __launch_bounds__(kMeanThreads, 10) neighbor_mean_kernel(MeanArgs a) {
-    __shared__ MeanShared sh;
-    dev::mean_sample(a, blockIdx.x * blockDim.x + threadIdx.x, sh.ranges[threadIdx.x >> 5]);
+__global__ void __launch_bounds__(128, 10) neighbor_mean_kernel(MeanArgs a) {
+    dev::mean_sample(a, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 __global__ void __launch_bounds__(256) scatter_kernel(ScatterArgs a) {
@@ -146,7 +145,7 @@ __global__ void positions_kernel(const float2* rec, const uint32_t* tag, uint32_
 
 void launch_neighbor_mean(const MeanArgs& a, cudaStream_t s) {
     if (a.n == 0) return;
-    neighbor_mean_kernel<<<div_up(a.n, kMeanThreads), kMeanThreads, 0, s>>>(a);
+    neighbor_mean_kernel<<<div_up(a.n, 128), 128, 0, s>>>(a);
 }
 
 void launch_scatter(const ScatterArgs& a, cudaStream_t s) {

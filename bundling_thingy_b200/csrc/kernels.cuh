@@ -83,22 +83,6 @@ cudaError_t launch_blur_vertical_tma(const float* in, float* out, uint32_t w, ui
 // it and biased by 2^30 so that the values are unsigned.
 constexpr uint32_t kFixedBias = 1u << 30;
 
-// Slot records carry this many spare entries past the last sample: the mean
-// kernel loads candidates in whole groups and masks those past a range's end.
-constexpr uint32_t kRecordPad = 8;
-
-// Neighbour-mean work layout (grid_dev.cuh): the search rows of a sample are
-// set up kMeanChunkRows at a time, in lockstep across the warp, into at most
-// two slot ranges per row kept in shared memory; then each lane walks its own
-// ranges, kMeanGroup candidate loads at a time.
-constexpr int kMeanChunkRows = 8;
-constexpr int kMeanRanges = 2 * kMeanChunkRows;
-constexpr int kMeanGroup = 4;
-constexpr int kMeanThreads = 128;
-// Shared memory of one mean CTA: the ranges of each lane, lane-interleaved.
-struct MeanShared {
-    uint2 ranges[kMeanThreads / 32][kMeanRanges][32];
-};
 
 __device__ __forceinline__ uint32_t biased_fixed(float v) {
     return static_cast<uint32_t>(__float2int_rn(v * kFixedScale)) + kFixedBias;
