@@ -278,8 +278,8 @@ bt_status enqueue_density(bt_ctx* c, uint32_t pass, cudaStream_t stream) {
     if (!blur_taps(sigma_for_pass(c->opt, pass), &taps)) return fail(c, BT_ERR_INVALID, "invalid blur sigma");
     // TMA-staged passes (blur_tma.cu) when the map's rows are whole 16-byte
     // units; element-staged ones (density.cu) otherwise. Same results.
-    const bool tma = bt::blur_tma_eligible(c->counts.p, c->himg.p, c->map.w, c->map.h) &&
-                     bt::blur_tma_eligible(c->himg.p, c->vimg.p, c->map.w, c->map.h);
+    const bool tma = bt::blur_tma_eligible(c->counts.p, c->himg.p, c->map.w, c->map.h, taps.R) &&
+                     bt::blur_tma_eligible(c->himg.p, c->vimg.p, c->map.w, c->map.h, taps.R);
     stage_begin(c, "density.blur_horizontal", stream);
     if (tma) {
         BT_CUDA(c, bt::launch_blur_horizontal_tma(c->counts.as<uint32_t>(), c->himg.as<float>(), c->map.w, c->map.h,

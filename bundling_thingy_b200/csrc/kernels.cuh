@@ -67,14 +67,16 @@ void launch_blur_horizontal(const uint32_t* counts, float* out, uint32_t w, uint
 void launch_blur_vertical(const float* in, float* out, uint32_t w, uint32_t h, const Taps& taps, uint32_t* peak,
                           cudaStream_t s);
 void launch_normalize(const float* in, const uint32_t* peak, float* out, size_t n, cudaStream_t s);
-// TMA-staged passes (blur_tma.cu), for maps whose rows are whole 16-byte units
-// and 16-byte aligned buffers (blur_tma_eligible); same results as the
-// element-staged passes. A copy wait that runs out sets bit 16 of *status.
-bool blur_tma_eligible(const void* in, const void* out, uint32_t w, uint32_t h);
+// TMA-staged passes (blur_tma.cu), for maps whose rows and columns are whole
+// 16-byte units, 16-byte aligned buffers and halos up to 48 texels
+// (blur_tma_eligible); same results as the element-staged passes. The
+// horizontal pass writes its result transposed (out_t[x * h + y]) and the
+// vertical pass reads it so. A copy wait that runs out sets bit 16 of *status.
+bool blur_tma_eligible(const void* in, const void* out, uint32_t w, uint32_t h, int R);
 cudaError_t prepare_blur_tma_kernels();
-cudaError_t launch_blur_horizontal_tma(const uint32_t* counts, float* out, uint32_t w, uint32_t h, const Taps& taps,
-                                       uint32_t* status, cudaStream_t s);
-cudaError_t launch_blur_vertical_tma(const float* in, float* out, uint32_t w, uint32_t h, const Taps& taps,
+cudaError_t launch_blur_horizontal_tma(const uint32_t* counts, float* out_t, uint32_t w, uint32_t h,
+                                       const Taps& taps, uint32_t* status, cudaStream_t s);
+cudaError_t launch_blur_vertical_tma(const float* in_t, float* out, uint32_t w, uint32_t h, const Taps& taps,
                                      uint32_t* peak, uint32_t* status, cudaStream_t s);
 
 // ---- neighbour grid and mean (grid.cu) ----
