@@ -118,11 +118,11 @@ __device__ __forceinline__ float2 moved_or_fixed(const AdvectArgs& a, uint32_t j
 // neighbours (a third of the gradient gathers and divisions of evaluating
 // both neighbours per thread). Every lane of the grid's warps reaches the
 // splat (idle lanes past n too): it is warp-aggregated.
-// Six CTAs of 256 per SM (40 registers): the density gathers are latency-
-// bound, and 48 resident warps hide them better than 32 at 61 registers
-// (154.5 against 189.8 us per cold launch of the large workload; seven or
-// more spill).
-__global__ void __launch_bounds__(kAdvectBlock, 6) advect_kernel(AdvectArgs a) {
+// Eight CTAs of 256 per SM (32 registers, 20 bytes spilled): the density
+// gathers are latency-bound, and 64 resident warps hide them better than 32
+// at 61 registers (four CTAs: 0.252 ms per iteration of the large workload
+// with the density passes; six at 40 registers: 0.219; eight: 0.210).
+__global__ void __launch_bounds__(kAdvectBlock, 8) advect_kernel(AdvectArgs a) {
     __shared__ float2 adv[kAdvectBlock + 2];
     const uint32_t base = blockIdx.x * kAdvectBlock;
     const uint32_t i = base + threadIdx.x;
