@@ -421,3 +421,19 @@ def test_headless_distortion_report(oracle, tmp_path, capsys):
     assert abs(last["distortion"] - d) <= 1e-12 * d
     assert abs(last["rms_displacement_pixels"] - px) <= 1e-12 * px
     assert r_dev["geometry"]["active_samples"] == gpu.info().samples
+
+
+@pytest.mark.parametrize("size,sigma", [(1001, 8.0), (512, 20.0), (1600, 0.0)])
+def test_density_paths_with_and_without_tma(oracle, size, sigma):
+    # The context's blur passes are TMA-staged when the map's sides are
+    # multiples of 4 and the halo is at most 48 texels (sigma <= 16), and
+    # element-staged otherwise: an odd side, a wide halo, and the reference's
+    # sigma-6 table on its 1600^2 canvas all match the oracle bit for bit.
+    w = synthetic.small()
+    o = bt.Options(width=size, height=size, neighbor_radius=4, blur_sigma=sigma, record_neighbors=True)
+    gpu, ora = pair(oracle, w.xy, w.starts, o)
+    check_density(gpu, ora)
+    gpu.iterate(2)
+    ora.iterate(2)
+    check_points(gpu, ora)
+    check_density(gpu, ora)
