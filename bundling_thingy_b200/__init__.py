@@ -127,6 +127,7 @@ SIGNATURES = {
     "bt_set_wait_seconds": ([_vp, ctypes.c_float], ctypes.c_int32),
     "bt_read_points": ([_vp, _vp, ctypes.c_size_t], ctypes.c_int32),
     "bt_read_paths": ([_vp, _vp, ctypes.c_size_t], ctypes.c_int32),
+    "bt_restore_points": ([_vp, _vp, ctypes.c_size_t, ctypes.c_uint32], ctypes.c_int32),
     "bt_read_segments": ([_vp, _u32p, ctypes.c_size_t], ctypes.c_int32),
     "bt_read_edges": ([_vp, _f32p, ctypes.c_size_t], ctypes.c_int32),
     "bt_read_density": ([_vp, _f32p, ctypes.c_size_t], ctypes.c_int32),
@@ -439,6 +440,14 @@ class Gpu:
     def read_points(self) -> tuple[np.ndarray, np.ndarray]:
         rec = self.read_records().view(np.uint32).reshape(-1, 3)
         return rec[:, :2].copy().view(np.float32), rec[:, 2].copy()
+
+    def restore_points(self, records: np.ndarray, iterations: int) -> None:
+        """Resume from a checkpoint: `records` are the 12-byte records that
+        read_records returned after `iterations` iterations of this graph (it
+        must be uploaded again with the same options first); iterating on
+        then gives the results of an uninterrupted run."""
+        rec = np.ascontiguousarray(records).reshape(-1).view(np.uint8)
+        self._ck(library().bt_restore_points(self._h, rec.ctypes.data, rec.size, iterations))
 
     def read_paths(self) -> np.ndarray:
         n = self.info().paths

@@ -527,7 +527,7 @@ void bt_destroy(bt_ctx* c) {
                       &c->cell_start, &c->hist_tiles, &c->counts, &c->himg, &c->vimg, &c->norm, &c->peak,
                       &c->records, &c->integrals, &c->r_seg_count, &c->r_seg_off, &c->r_scan64,
                       &c->r_pair_tile, &c->r_pair_seg, &c->r_sorted, &c->r_hist, &c->r_hist_off, &c->r_scan32,
-                      &c->r_samples, &c->r_rgba, &c->r_misc, &c->adv_xy};
+                      &c->r_samples, &c->r_rgba, &c->r_misc, &c->adv_xy, &c->ckpt_tag};
     for (DevBuf* b : bufs) release(*b, c->stream);
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->account) c->account->used -= c->device_bytes;
@@ -1097,6 +1097,58 @@ bt_status bt_read_points(bt_ctx* c, void* dst, size_t bytes) {
     if (!dst || bytes != 12ull * c->samples) return fail(c, BT_ERR_INVALID, "point buffer must hold 12 bytes per sample");
     if (bt_status s = bt::prepare_records(c)) return s;
     return copy_out(c, dst, c->records.p, bytes);
+}
+
+bt_status bt_restore_points(bt_ctx* c, const void* records, size_t bytes, uint32_t iterations) {
+    if (bt_status s = need_graph(c)) return s;
+    if (!records || bytes != 12ull * c->samples)
+        return fail(c, BT_ERR_INVALID, "checkpoint must hold 12 bytes per sample of the uploaded graph");
+    const bool advect = c->opt.advect_step > 0.0f;
+    cudaSetDevice(c->device);
+    c->stage_used = 0;
+    if (bt_status s = ensure(c, c->records, bytes)) return s;
+    if (bt_status s = ensure(c, c->current, 8ull * c->samples)) return s;
+    if (c->has_grid)
+        if (bt_status s = ensure(c, c->ckpt_tag, 4ull * c->samples)) return s;
+    BT_CUDA(c, cudaMemsetAsync(c->status.p, 0, 4, c->stream));
+    BT_CUDA(c, cudaMemcpyAsync(c->records.p, records, bytes, cudaMemcpyHostToDevice, c->stream));
+    // Sample-order positions (and tags) into scratch, checked against the
+    // graph before anything the context iterates on changes.
+    float2* xy = c->current.as<float2>();
+    bt::launch_restore_records(c->records.as<uint32_t>(), c->edge_ids.as<uint32_t>(),
+                               c->has_grid ? c->sorted_tag[c->cur].as<uint32_t>() : nullptr, c->samples, xy,
+                               c->has_grid ? c->ckpt_tag.as<uint32_t>() : nullptr, c->status.as<uint32_t>(),
+                               c->stream);
+    BT_CUDA(c, cudaMemcpyAsync(c->h_status, c->status.p, 4, cudaMemcpyDeviceToHost, c->stream));
+    if (bt_status s = wait(c)) return s;
+    if (c->h_status[0] & 32u)
+        return fail(c, BT_ERR_INVALID, "checkpoint does not match the uploaded graph (edge ids or positions)");
+    if (advect) {
+        // The advection mode iterates on sample-order positions.
+        BT_CUDA(c, cudaMemcpyAsync(c->tmp_xy.p, xy, 8ull * c->samples, cudaMemcpyDeviceToDevice, c->stream));
+        xy = c->tmp_xy.as<float2>();
+    }
+    if (c->has_grid) {
+        // Bin the positions for the next iteration, as after a mean step.
+        BT_CUDA(c, cudaMemsetAsync(c->hist.p, 0, c->cells * 4, c->stream));
+        bt::launch_rebin(xy, c->ckpt_tag.as<uint32_t>(), c->samples, c->grid, c->tmp_xy.as<float2>(),
+                         c->tmp_tag.as<uint32_t>(), c->tmp_cell.as<uint32_t>(), c->hist.as<uint32_t>(), c->stream);
+        enqueue_binning(c, c->cur ^ 1, false);
+        c->cur ^= 1;
+    }
+    // The density of the restored positions: pass `iterations`, as the
+    // iteration that produced them ran it.
+    const bool density = advect || c->accumulate;
+    if (density) {
+        BT_CUDA(c, cudaMemsetAsync(c->counts.p, 0, c->texels * sizeof(uint32_t), c->stream));
+        BT_CUDA(c, cudaMemsetAsync(c->peak.p, 0, sizeof(uint32_t), c->stream));
+        bt::launch_splat_positions(xy, c->samples, c->map, c->counts.as<uint32_t>(), c->stream);
+        if (bt_status s = enqueue_density(c, iterations, c->stream)) return s;
+    }
+    c->iterations = iterations;
+    c->density_passes = density ? iterations + 1 : 0;
+    BT_CUDA(c, cudaGetLastError());
+    return check_iteration_status(c);
 }
 
 bt_status bt_read_paths(bt_ctx* c, void* dst, size_t bytes) {

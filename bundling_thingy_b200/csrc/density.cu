@@ -61,7 +61,19 @@ __global__ void normalize_tail_kernel(const float* in, const uint32_t* peak_bits
     if (i < n) out[i] = dev::normalized_value(in[i], peak);
 }
 
+__global__ void splat_positions_kernel(const float2* xy, uint32_t n, Map map, uint32_t* counts) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float2 p = xy[i];
+    uint32_t d;
+    if (splat_index(p.x, p.y, map, &d)) atomicAdd(&counts[d], 1u);
+}
+
 }  // namespace
+
+void launch_splat_positions(const float2* xy, uint32_t n, Map map, uint32_t* counts, cudaStream_t s) {
+    if (n) splat_positions_kernel<<<div_up(n, 256), 256, 0, s>>>(xy, n, map, counts);
+}
 
 // Opt the blur kernels into the shared memory of the widest tap count
 // (R = 128). Called once per device before any launch or graph capture.

@@ -141,7 +141,29 @@ __global__ void positions_kernel(const float2* rec, const uint32_t* tag, uint32_
     out[tag[s] & ~kMovableBit] = rec[s];
 }
 
+__global__ void restore_kernel(const uint32_t* records, const uint32_t* edge_ids, const uint32_t* slot_tag, uint32_t n,
+                               float2* xy, uint32_t* tag_out, uint32_t* status) {
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    uint32_t i = s;
+    if (slot_tag) {
+        const uint32_t t = slot_tag[s];
+        i = t & ~kMovableBit;
+        tag_out[i] = t;
+    }
+    const float x = __uint_as_float(records[3 * static_cast<size_t>(i)]);
+    const float y = __uint_as_float(records[3 * static_cast<size_t>(i) + 1]);
+    if (records[3 * static_cast<size_t>(i) + 2] != edge_ids[i] || !isfinite(x) || !isfinite(y)) atomicOr(status, 32u);
+    xy[i] = make_float2(x, y);
+}
+
 }  // namespace
+
+void launch_restore_records(const uint32_t* records, const uint32_t* edge_ids, const uint32_t* slot_tag, uint32_t n,
+                            float2* xy, uint32_t* tag_out, uint32_t* status, cudaStream_t s) {
+    if (n == 0) return;
+    restore_kernel<<<div_up(n, 256), 256, 0, s>>>(records, edge_ids, slot_tag, n, xy, tag_out, status);
+}
 
 void launch_neighbor_mean(const MeanArgs& a, cudaStream_t s) {
     if (a.n == 0) return;

@@ -165,6 +165,15 @@ void launch_records_from_sample_order(const float2* xy, const uint32_t* edge_ids
 void launch_grid_cells(const float2* rec, const uint32_t* tag, uint32_t n, const Grid& g, uint32_t* out,
                        cudaStream_t s);
 void launch_positions_from_slots(const float2* rec, const uint32_t* tag, uint32_t n, float2* out, cudaStream_t s);
+// Checkpointed 12-byte {x, y, edge_id} records (sample order) back into
+// sample-order positions; with slot_tag (the current slot order's tags) also
+// each sample's tag in sample order (tag_out). A record whose edge id differs
+// from the uploaded graph's, or whose position is not finite, sets bit 5
+// (value 32) of *status.
+void launch_restore_records(const uint32_t* records, const uint32_t* edge_ids, const uint32_t* slot_tag, uint32_t n,
+                            float2* xy, uint32_t* tag_out, uint32_t* status, cudaStream_t s);
+// Density splat of n sample positions (counts zero before the launch).
+void launch_splat_positions(const float2* xy, uint32_t n, Map map, uint32_t* counts, cudaStream_t s);
 
 // ---- distortion (distortion.cu) ----
 // Per-edge squared_integral of original vs current (sample order); status bit

@@ -160,6 +160,16 @@ bt_status bt_set_wait_seconds(bt_ctx* ctx, float seconds);
 /* 12-byte little-endian {f32 x, f32 y, u32 edge_id} records, sample order
  * (the point buffer read by distortion_snapshot, src/gpu.rs:469-482). */
 bt_status bt_read_points(bt_ctx* ctx, void* dst, size_t bytes);
+/* Checkpoint/resume (beyond the reference, whose bundling state is the point
+ * buffer that distortion_snapshot reads, src/gpu.rs:469-482): bt_read_points
+ * gives the checkpoint; this puts its positions back into the uploaded graph
+ * (the same graph and options, after bt_upload) as the state after
+ * `iterations` iterations: the positions are re-binned for the next
+ * iteration and their density recomputed with that iteration's density pass,
+ * so iterating on gives the same results as an uninterrupted run. Records
+ * whose edge ids differ from the uploaded graph's, or whose positions are
+ * not finite, are refused with BT_ERR_INVALID. */
+bt_status bt_restore_points(bt_ctx* ctx, const void* records, size_t bytes, uint32_t iterations);
 /* 12-byte {u32 point_offset, u32 segment_offset, u32 count} per edge
  * (distortion_layout, src/gpu.rs:438-467). Skipped edges read as zeros. */
 bt_status bt_read_paths(bt_ctx* ctx, void* dst, size_t bytes);
