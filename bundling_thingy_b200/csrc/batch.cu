@@ -804,6 +804,7 @@ bt_status bt_batch_remove(bt_batch* b, uint32_t slot) {
 }
 
 bt_status bt_batch_iterate_async(bt_batch* b, uint32_t n) {
+    NvtxRange range("batch_iterate");
     if (!b) return bfail(nullptr, BT_ERR_INVALID, "null batch");
     cudaSetDevice(b->device);
     bool any = false, any_solo = false;

@@ -868,6 +868,7 @@ extern "C" {
 
 bt_status bt_upload(bt_ctx* c, const float* xy, uint32_t n_points, const uint32_t* starts, uint32_t n_starts,
                     uint32_t* out_samples) {
+    bt::NvtxRange range("Gpu::upload");
     if (!out_samples) return fail(c, BT_ERR_INVALID, "null argument");
     if (bt_status s = bt::upload_begin(c, xy, n_points, starts, n_starts)) return s;
     if (bt_status s = wait(c)) return s;
@@ -884,6 +885,7 @@ bt_status bt_upload_graph(bt_ctx* c, const bt_graph* g, uint32_t* out_samples) {
 }
 
 bt_status bt_iterate_async(bt_ctx* c, uint32_t n) {
+    bt::NvtxRange range("Gpu::iterate");
     if (!c) return fail(nullptr, BT_ERR_INVALID, "null context");
     const bool advect = c->opt.advect_step > 0.0f;
     if (!c->has_grid && !advect) return fail(c, BT_ERR_NOT_CONFIGURED, "neighbor radius is not configured");
@@ -1100,6 +1102,7 @@ bt_status bt_read_points(bt_ctx* c, void* dst, size_t bytes) {
 }
 
 bt_status bt_restore_points(bt_ctx* c, const void* records, size_t bytes, uint32_t iterations) {
+    bt::NvtxRange range("restore_points");
     if (bt_status s = need_graph(c)) return s;
     if (!records || bytes != 12ull * c->samples)
         return fail(c, BT_ERR_INVALID, "checkpoint must hold 12 bytes per sample of the uploaded graph");
@@ -1234,6 +1237,7 @@ bt_status bt_read_neighbors(bt_ctx* c, uint32_t* dst, size_t count) {
 }
 
 bt_status bt_distortion(bt_ctx* c, uint32_t size, double* distortion, double* rms_px) {
+    bt::NvtxRange range("distortion");
     if (bt_status s = need_graph(c)) return s;
     if (!c->opt.evaluate_distortion) return fail(c, BT_ERR_NOT_CONFIGURED, "distortion staging disabled");
     if (!distortion || !rms_px || size == 0) return fail(c, BT_ERR_INVALID, "distortion viewport must be nonzero");
@@ -1355,6 +1359,7 @@ bt_status render_frame(bt_ctx* c, const float2* xy, bool timed, uint8_t* rgba, u
 }  // namespace
 
 bt_status bt_render(bt_ctx* c, uint8_t* rgba, size_t rgba_bytes, uint64_t* colored_pixels, float* device_ms) {
+    bt::NvtxRange range("Gpu::render");
     if (!c) return fail(nullptr, BT_ERR_INVALID, "null context");
     cudaSetDevice(c->device);
     const size_t pixels = static_cast<size_t>(c->opt.width) * c->opt.height;

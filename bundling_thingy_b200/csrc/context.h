@@ -10,11 +10,24 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "bt.h"
 #include "host.h"
 #include "kernels.cuh"
 
 namespace bt {
+
+// An NVTX range over a public call (named after the reference's `Gpu`
+// method it replaces), for timelines of profilers; without one attached the
+// NVTX calls do nothing.
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
+
 
 struct DevBuf {
     void* p = nullptr;
