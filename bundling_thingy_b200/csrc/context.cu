@@ -352,6 +352,7 @@ bt_status enqueue_iteration(bt_ctx* c, int src, uint32_t pass) {
     m.hist_tiles = c->hist_tiles.as<uint32_t>();
     m.counts = c->accumulate ? c->counts.as<uint32_t>() : nullptr;
     m.neighbors = c->opt.record_neighbors ? c->neighbors.as<uint32_t>() : nullptr;
+    m.chunk_counter = c->chunk_counter.as<uint32_t>();
     m.n = c->samples;
     m.g = c->grid;
     bt::launch_neighbor_mean(m, c->stream);
@@ -527,7 +528,7 @@ void bt_destroy(bt_ctx* c) {
                       &c->cell_start, &c->hist_tiles, &c->counts, &c->himg, &c->vimg, &c->norm, &c->peak,
                       &c->records, &c->integrals, &c->r_seg_count, &c->r_seg_off, &c->r_scan64,
                       &c->r_pair_tile, &c->r_pair_seg, &c->r_sorted, &c->r_hist, &c->r_hist_off, &c->r_scan32,
-                      &c->r_samples, &c->r_rgba, &c->r_misc, &c->adv_xy, &c->ckpt_tag};
+                      &c->r_samples, &c->r_rgba, &c->r_misc, &c->adv_xy, &c->ckpt_tag, &c->chunk_counter};
     for (DevBuf* b : bufs) release(*b, c->stream);
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->account) c->account->used -= c->device_bytes;
@@ -626,6 +627,7 @@ bt_status bt::create_context(const bt_options* options, bt::MemAccount* account,
     if (bt_status s = ensure(c, c->peak, 16)) return bail(s);
     if (bt_status s = ensure(c, c->totals, 32)) return bail(s);
     if (bt_status s = ensure(c, c->status, 16)) return bail(s);
+    if (bt_status s = ensure(c, c->chunk_counter, 16)) return bail(s);
     cudaMemsetAsync(c->counts.p, 0, c->texels * 4, c->stream);
     cudaMemsetAsync(c->vimg.p, 0, c->texels * 4, c->stream);
     cudaMemsetAsync(c->norm.p, 0, c->texels * 4, c->stream);

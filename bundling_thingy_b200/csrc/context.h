@@ -131,6 +131,7 @@ struct bt_ctx {
     bt::DevBuf records, integrals;
     bt::DevBuf adv_xy;                          // advection mode: next positions, sample order
     bt::DevBuf ckpt_tag;                        // bt_restore_points: tags in sample order
+    bt::DevBuf chunk_counter;                   // the mean kernel's work-queue head
     // bt_render: tile bins, samples, image, and {colored pixels, pairs}.
     bt::DevBuf r_seg_count, r_seg_off, r_scan64, r_pair_tile, r_pair_seg, r_sorted, r_hist, r_hist_off, r_scan32;
     bt::DevBuf r_samples, r_rgba, r_misc;

@@ -107,6 +107,7 @@ struct MeanArgs {
     uint32_t* hist_tiles;    // their sums per cell-table tile (zero before the launch)
     uint32_t* counts;        // density splat (nullptr = off)
     uint32_t* neighbors;     // |N(p)| per slot (nullptr = off)
+    uint32_t* chunk_counter; // work-queue head of the persistent single-graph kernel (reset by its launcher)
     uint32_t n;
     Grid g;
     int mode;                // SearchMode
