@@ -199,19 +199,24 @@ void set_search_shape(bt::Grid& g, uint32_t ky, uint32_t kx) {
 // sample (samples per texel^2), a search costs about 2r / sy row lookups plus
 // rho 4r (sy + sx) exact tests per sample, and the cell table about 8 bytes a
 // cell per iteration: the best row height goes as 1 / sqrt(rho), and cells
-// about 8 times narrower than high pay for their table. The constants are
-// fitted to timings of whole iterations on B200 (after 8 iterations, over
-// graphs of 0.3 to 30 samples per texel^2 at upload, radius 4 to 16).
+// about 8 times narrower than high pay for their table. The constant 2.7 is
+// fitted on B200 to the first ten iterations after an upload, which hold a
+// job's costliest iterations. Per-iteration timings of 4 to 6 shapes on each
+// of seven graphs (radius 2 to 16, 0.6M to 12M samples, maps of 256^2 to
+// 2048^2) put the fastest rows 1.5 to 2 times lower than 4.5 / sqrt(rho),
+// with little change beyond. The earlier constant 4.5 was fitted after the
+// eighth iteration. It was 8 to 12% slower on the ten-iteration jobs and
+// equal on a 30-iteration job of 5M samples.
 void adaptive_shape(const bt_ctx* c, unsigned long long pairs, uint32_t* ky_out, uint32_t* kx_out) {
     const bt::Grid& g = c->grid;
     const double r = g.rf, n = static_cast<double>(c->samples);
     const double rho = std::max(static_cast<double>(pairs) / (r * r * n), 1e-4);
-    const double sy = std::min(std::max(4.5 / std::sqrt(rho), 0.25), std::min(4.0, r));
+    const double sy = std::min(std::max(2.7 / std::sqrt(rho), 0.25), std::min(4.0, r));
     uint32_t ky = static_cast<uint32_t>(std::min(std::max(std::lround(r / sy), 1L), 4096L));
     uint32_t kx = std::min(8u * ky, 4096u);
-    // At most 32 Mi search cells (8 bytes each per iteration) and 8 per sample.
+    // At most 64 Mi search cells (8 bytes each per iteration) and 8 per sample.
     const uint64_t grid_cells = static_cast<uint64_t>(g.gw) * g.gh;
-    const uint64_t cap = std::min<uint64_t>(32ull << 20, std::max<uint64_t>(grid_cells, 8ull * c->samples));
+    const uint64_t cap = std::min<uint64_t>(64ull << 20, std::max<uint64_t>(grid_cells, 8ull * c->samples));
     if (grid_cells * ky * kx > cap) kx = static_cast<uint32_t>(std::max<uint64_t>(ky, cap / (grid_cells * ky)));
     if (grid_cells * ky * kx > cap)
         ky = kx = static_cast<uint32_t>(std::max(1.0, std::floor(std::sqrt(static_cast<double>(cap) / grid_cells))));
