@@ -210,13 +210,13 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum: 86.67 + 46.70 MB)
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum: 99.60 + 49.79 MB)
 # of one launch of the neighbour-mean kernel on the large workload, iteration
 # 15 of a job, from one ncu capture (1 pass) of this kernel on B200:
 #   ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum \
 #       --clock-control none -k regex:neighbor_mean -s 14 -c 1 \
 #       python bench.py --quick --steps 1 --warmup 0 --steady-iterations 0
-MEAN_TRAFFIC_BYTES = 133_370_000
+MEAN_TRAFFIC_BYTES = 149_390_000
 
 
 def workload(edges: int):
