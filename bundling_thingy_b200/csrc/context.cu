@@ -173,6 +173,9 @@ double sigma_for_pass(const bt_options& o, uint32_t pass) {
 // Search-cell shape chosen per graph (the options fix none).
 bool adaptive(const bt_ctx* c) { return c->opt.fine_cells == 0 && c->opt.fine_cells_x == 0; }
 
+// Iteration count of a graph's first search-shape check (check_shape).
+constexpr uint32_t kFirstShapeCheck = 5;
+
 bool constant_sigma(const bt_options& o) {
     return o.blur_sigma == 0.0f || o.blur_shrink == 0.0f || o.blur_shrink == 1.0f;
 }
@@ -207,11 +210,20 @@ void set_search_shape(bt::Grid& g, uint32_t ky, uint32_t kx) {
 // with little change beyond. The earlier constant 4.5 was fitted after the
 // eighth iteration. It was 8 to 12% slower on the ten-iteration jobs and
 // equal on a 30-iteration job of 5M samples.
+void shape_for_rows(const bt_ctx* c, double sy, uint32_t* ky_out, uint32_t* kx_out);
+
 void adaptive_shape(const bt_ctx* c, unsigned long long pairs, uint32_t* ky_out, uint32_t* kx_out) {
-    const bt::Grid& g = c->grid;
-    const double r = g.rf, n = static_cast<double>(c->samples);
+    const double r = c->grid.rf, n = static_cast<double>(c->samples);
     const double rho = std::max(static_cast<double>(pairs) / (r * r * n), 1e-4);
-    const double sy = std::min(std::max(2.7 / std::sqrt(rho), 0.25), std::min(4.0, r));
+    shape_for_rows(c, 2.7 / std::sqrt(rho), ky_out, kx_out);
+}
+
+// Search cells of rows about sy texels high (at least 1/4 texel, at most
+// min(4, r)), 8 times narrower than high.
+void shape_for_rows(const bt_ctx* c, double sy, uint32_t* ky_out, uint32_t* kx_out) {
+    const bt::Grid& g = c->grid;
+    const double r = g.rf;
+    sy = std::min(std::max(sy, 0.25), std::min(4.0, r));
     uint32_t ky = static_cast<uint32_t>(std::min(std::max(std::lround(r / sy), 1L), 4096L));
     uint32_t kx = std::min(8u * ky, 4096u);
     // At most 64 Mi search cells (8 bytes each per iteration) and 8 per sample.
@@ -533,7 +545,8 @@ void bt_destroy(bt_ctx* c) {
                       &c->cell_start, &c->hist_tiles, &c->counts, &c->himg, &c->vimg, &c->norm, &c->peak,
                       &c->records, &c->integrals, &c->r_seg_count, &c->r_seg_off, &c->r_scan64,
                       &c->r_pair_tile, &c->r_pair_seg, &c->r_sorted, &c->r_hist, &c->r_hist_off, &c->r_scan32,
-                      &c->r_samples, &c->r_rgba, &c->r_misc, &c->adv_xy, &c->ckpt_tag, &c->chunk_counter};
+                      &c->r_samples, &c->r_rgba, &c->r_misc, &c->adv_xy, &c->ckpt_tag, &c->chunk_counter,
+                      &c->probe};
     for (DevBuf* b : bufs) release(*b, c->stream);
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->account) c->account->used -= c->device_bytes;
@@ -633,6 +646,7 @@ bt_status bt::create_context(const bt_options* options, bt::MemAccount* account,
     if (bt_status s = ensure(c, c->totals, 32)) return bail(s);
     if (bt_status s = ensure(c, c->status, 16)) return bail(s);
     if (bt_status s = ensure(c, c->chunk_counter, 16)) return bail(s);
+    if (bt_status s = ensure(c, c->probe, 32)) return bail(s);
     cudaMemsetAsync(c->counts.p, 0, c->texels * 4, c->stream);
     cudaMemsetAsync(c->vimg.p, 0, c->texels * 4, c->stream);
     cudaMemsetAsync(c->norm.p, 0, c->texels * 4, c->stream);
@@ -657,6 +671,7 @@ bt_status bt::upload_begin(bt_ctx* c, const float* xy, uint32_t n_points, const 
     c->uploaded = false;
     c->samples = 0;
     c->iterations = 0;
+    c->next_shape_check = kFirstShapeCheck;
     c->density_passes = 0;
     // The iteration graphs are refreshed at the next iteration (an update of
     // the executable graph when the new capture has the same shape).
@@ -811,10 +826,19 @@ bt_status bt::upload_finish(bt_ctx* c) {
     return BT_OK;
 }
 
+bt_status reshape(bt_ctx* c, uint32_t ky, uint32_t kx);
+
 bt_status bt::upload_adapt(bt_ctx* c) {
     if (!c->has_grid || !adaptive(c) || c->samples == 0) return BT_OK;
     uint32_t ky = 0, kx = 0;
     adaptive_shape(c, c->h_totals[2], &ky, &kx);
+    return reshape(c, ky, kx);
+}
+
+// Re-bins the current slot order under ky x kx search cells per grid cell
+// (every shape gives the same neighbour sets and sums). When an allocation is
+// refused (a memory budget), the graph keeps the shape it has.
+bt_status reshape(bt_ctx* c, uint32_t ky, uint32_t kx) {
     if (ky == c->grid.ky && kx == c->grid.kx) return BT_OK;
     bt::Grid g = c->grid;
     set_search_shape(g, ky, kx);
@@ -828,6 +852,7 @@ bt_status bt::upload_adapt(bt_ctx* c) {
     if (!room) return BT_OK;
     c->grid = g;
     c->cells = cells;
+    c->graph_stale[0] = c->graph_stale[1] = true;   // their kernels hold the old grid
     stage_begin(c, "graph.rebin");
     bt::launch_rebin(c->sorted_rec[c->cur].as<float2>(), c->sorted_tag[c->cur].as<uint32_t>(), c->samples, c->grid,
                      c->tmp_xy.as<float2>(), c->tmp_tag.as<uint32_t>(), c->tmp_cell.as<uint32_t>(),
@@ -836,6 +861,49 @@ bt_status bt::upload_adapt(bt_ctx* c) {
     enqueue_binning(c, c->cur ^ 1, false);
     c->cur ^= 1;
     return BT_OK;
+}
+
+// Search-shape checks during a job. Early iterations test many boundary
+// samples per search row and favour low rows; as a graph bundles its
+// boundary bands empty, the rows dominate and tall rows win (on the large
+// workload 2-texel rows are fastest at first and 4-texel rows from about the
+// tenth iteration). After 5, 10, 20, 40, ... iterations of an upload, the
+// synchronous calls (bt_iterate, bt_iterate_timed) count the search rows and
+// the boundary samples of every 16th slot under the current shape, predict
+// the best row height and re-bin when the prediction saves more than 8%.
+// The cost model: per sample, kRowCost exact tests' worth per search row
+// (about 2R / sy + 1 rows) plus the boundary samples, whose count scales with
+// the band's width sy + sx. kRowCost is fitted to per-iteration times of five
+// shapes on the large workload at iterations 1 and 30.
+constexpr uint32_t kProbeStride = 16;
+constexpr double kRowCost = 10.0;
+constexpr double kReshapeGain = 0.92;
+
+bt_status check_shape(bt_ctx* c) {
+    c->next_shape_check = std::max(c->iterations, kFirstShapeCheck) * 2u;
+    if (!c->has_grid || !adaptive(c) || c->samples == 0) return BT_OK;
+    bt::launch_search_probe(c->sorted_rec[c->cur].as<float2>(), c->sorted_tag[c->cur].as<uint32_t>(),
+                            c->cell_start.as<uint32_t>(), c->samples, c->grid, kProbeStride,
+                            c->probe.as<unsigned long long>(), c->stream);
+    BT_CUDA(c, cudaMemcpyAsync(c->h_totals + 5, c->probe.p, 24, cudaMemcpyDeviceToHost, c->stream));
+    // A check is only an optimisation: past the wait deadline the call goes
+    // on without it (the queued work completes, as for any expired wait).
+    if (bt_status s = wait(c)) return s == BT_ERR_TIMEOUT ? BT_OK : s;
+    const double probed = static_cast<double>(c->h_totals[7]);
+    if (probed < 64.0) return BT_OK;
+    const double tests = static_cast<double>(c->h_totals[6]) / probed;
+    const bt::Grid& g = c->grid;
+    const double R = static_cast<double>(g.rf) + g.margin;
+    const double band = static_cast<double>(g.sy) + g.sx;
+    auto cost = [&](double sy, double sx) { return kRowCost * (2.0 * R / sy + 1.0) + tests * (sy + sx) / band; };
+    // Minimum of kRowCost 2R / sy + tests (sy + sy / 8) / band.
+    const double sy_best = std::sqrt(2.0 * R * kRowCost * band / (1.125 * std::max(tests, 1e-3)));
+    uint32_t ky = 0, kx = 0;
+    shape_for_rows(c, sy_best, &ky, &kx);
+    if (ky == g.ky && kx == g.kx) return BT_OK;
+    const double sy_new = static_cast<double>(g.rf) / ky, sx_new = static_cast<double>(g.rf) / kx;
+    if (cost(sy_new, sx_new) > kReshapeGain * cost(g.sy, g.sx)) return BT_OK;
+    return reshape(c, ky, kx);
 }
 
 bt_status bt::upload_check(bt_ctx* c, uint32_t* out_samples) {
@@ -891,14 +959,16 @@ bt_status bt_upload_graph(bt_ctx* c, const bt_graph* g, uint32_t* out_samples) {
                      static_cast<uint32_t>(g->g.starts.size()), out_samples);
 }
 
-bt_status bt_iterate_async(bt_ctx* c, uint32_t n) {
+// Enqueues n iterations; reset_stages starts a new set of stage records
+// (timing mode), otherwise they add to the current one.
+bt_status iterate_enqueue(bt_ctx* c, uint32_t n, bool reset_stages) {
     bt::NvtxRange range("Gpu::iterate");
     if (!c) return fail(nullptr, BT_ERR_INVALID, "null context");
     const bool advect = c->opt.advect_step > 0.0f;
     if (!c->has_grid && !advect) return fail(c, BT_ERR_NOT_CONFIGURED, "neighbor radius is not configured");
     if (!c->uploaded) return fail(c, BT_ERR_NO_GRAPH, "no uploaded graph");
     cudaSetDevice(c->device);
-    c->stage_used = 0;
+    if (reset_stages) c->stage_used = 0;
     if (advect) {
         if (bt_status s = ensure(c, c->adv_xy, 8ull * c->samples)) return s;
         for (uint32_t i = 0; i < n; ++i) {
@@ -984,8 +1054,28 @@ bt_status check_iteration_status(bt_ctx* c) {
 }
 }  // namespace
 
+bt_status bt_iterate_async(bt_ctx* c, uint32_t n) { return iterate_enqueue(c, n, true); }
+
+// bt_iterate_async in pieces, with the search-shape checks that fall due
+// on the way (check_shape).
+bt_status iterate_checked(bt_ctx* c, uint32_t n) {
+    if (!c || !c->uploaded) return iterate_enqueue(c, n, true);   // its errors
+    const bool checks = c->has_grid && c->opt.advect_step <= 0.0f && adaptive(c);
+    c->stage_used = 0;
+    if (n == 0) return iterate_enqueue(c, 0, false);
+    while (n > 0) {
+        if (checks && c->next_shape_check && c->iterations >= c->next_shape_check)
+            if (bt_status s = check_shape(c)) return s;
+        uint32_t chunk = n;
+        if (checks && c->next_shape_check > c->iterations) chunk = std::min(n, c->next_shape_check - c->iterations);
+        if (bt_status s = iterate_enqueue(c, chunk, false)) return s;
+        n -= chunk;
+    }
+    return BT_OK;
+}
+
 bt_status bt_iterate(bt_ctx* c, uint32_t n) {
-    if (bt_status s = bt_iterate_async(c, n)) return s;
+    if (bt_status s = iterate_checked(c, n)) return s;
     return check_iteration_status(c);
 }
 
@@ -997,7 +1087,7 @@ bt_status bt_iterate_timed(bt_ctx* c, uint32_t n, float* device_ms) {
         BT_CUDA(c, cudaEventCreate(&c->t1));
     }
     BT_CUDA(c, cudaEventRecord(c->t0, c->stream));
-    if (bt_status s = bt_iterate_async(c, n)) return s;
+    if (bt_status s = iterate_checked(c, n)) return s;
     BT_CUDA(c, cudaEventRecord(c->t1, c->stream));
     if (bt_status s = wait(c)) return s;
     BT_CUDA(c, cudaEventElapsedTime(device_ms, c->t0, c->t1));
@@ -1156,6 +1246,7 @@ bt_status bt_restore_points(bt_ctx* c, const void* records, size_t bytes, uint32
         if (bt_status s = enqueue_density(c, iterations, c->stream)) return s;
     }
     c->iterations = iterations;
+    c->next_shape_check = std::max(iterations, kFirstShapeCheck);
     c->density_passes = density ? iterations + 1 : 0;
     BT_CUDA(c, cudaGetLastError());
     return check_iteration_status(c);

@@ -132,6 +132,7 @@ struct bt_ctx {
     bt::DevBuf adv_xy;                          // advection mode: next positions, sample order
     bt::DevBuf ckpt_tag;                        // bt_restore_points: tags in sample order
     bt::DevBuf chunk_counter;                   // the mean kernel's work-queue head
+    bt::DevBuf probe;                           // sampled search work (rows, boundary samples, probed)
     // bt_render: tile bins, samples, image, and {colored pixels, pairs}.
     bt::DevBuf r_seg_count, r_seg_off, r_scan64, r_pair_tile, r_pair_seg, r_sorted, r_hist, r_hist_off, r_scan32;
     bt::DevBuf r_samples, r_rgba, r_misc;
@@ -146,6 +147,7 @@ struct bt_ctx {
     uint32_t samples = 0, n_paths = 0, drawn = 0, capacity = 0;
     uint64_t reserved_bytes = 0;
     uint32_t iterations = 0, density_passes = 0;
+    uint32_t next_shape_check = 0;              // iteration count of the next search-shape check (0: none)
     int cur = 0;
 
     cudaGraphExec_t graphs[2] = {nullptr, nullptr};

@@ -188,6 +188,72 @@ void launch_neighbor_mean(const MeanArgs& a, cudaStream_t s) {
     neighbor_mean_kernel<<<grid, 128, 0, s>>>(a);
 }
 
+// Work of the neighbour search on every `stride`-th slot: its search rows
+// and the samples of its boundary cells (those the mean tests exactly), with
+// the row bounds of mean_sample. out[0] += rows, out[1] += boundary samples,
+// out[2] += movable samples probed.
+__global__ void __launch_bounds__(256) search_probe_kernel(const float2* rec, const uint32_t* tag,
+                                                           const uint32_t* cell_start, uint32_t n, Grid g,
+                                                           uint32_t stride, unsigned long long* out) {
+    const uint64_t s = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) * stride;
+    uint32_t rows = 0, tests = 0, probed = 0;
+    if (s < n && (tag[s] & kMovableBit)) {
+        const float2 p = rec[s];
+        const float tx = texel_of(p.x, g.map.wm1), ty = texel_of(p.y, g.map.hm1);
+        const uint32_t cx0 = grid_of(tx - g.reachx, g.rf, g.gw), cx1 = grid_of(tx + g.reachx, g.rf, g.gw);
+        const uint32_t cy0 = grid_of(ty - g.reachy, g.rf, g.gh), cy1 = grid_of(ty + g.reachy, g.rf, g.gh);
+        const int fx_min = static_cast<int>(cx0 * g.kx), fx_max = static_cast<int>(cx1 * g.kx + g.kx - 1u);
+        const int fy_min = static_cast<int>(cy0 * g.ky), fy_max = static_cast<int>(cy1 * g.ky + g.ky - 1u);
+        const float R = g.rf + g.margin, Rin = g.rf - g.margin;
+        const int fw = static_cast<int>(g.fw), fh = static_cast<int>(g.fh);
+        const int fy_lo = max(fy_min, static_cast<int>(floorf((ty - R) * g.inv_sy)));
+        const int fy_hi = min(fy_max, static_cast<int>(floorf((ty + R) * g.inv_sy)));
+        probed = 1;
+        for (int fy = fy_lo; fy <= fy_hi; ++fy) {
+            const float ylo = static_cast<float>(fy) * g.sy, yhi = ylo + g.sy;
+            const float dn = fmaxf(fmaxf(fmaxf(ylo - ty, ty - yhi), 0.0f) - g.margin, 0.0f);
+            if (dn > R) continue;
+            const float hout = sqrtf(fmaxf(R * R - dn * dn, 0.0f)) + g.margin;
+            const int bx0 = max(fx_min, static_cast<int>(floorf((tx - hout) * g.inv_sx)));
+            const int bx1 = min(fx_max, static_cast<int>(floorf((tx + hout) * g.inv_sx)));
+            if (bx0 > bx1) continue;
+            ++rows;
+            const uint32_t row = static_cast<uint32_t>(fy) * g.fw;
+            const uint32_t s0 = cell_start[row + bx0], s3 = cell_start[row + bx1 + 1];
+            uint32_t inner = 0;
+            const float far = fmaxf(fabsf(ylo - ty), fabsf(yhi - ty)) + g.margin;
+            if (fy > 0 && fy < fh - 1 && far < Rin) {
+                const float hin = sqrtf(fmaxf(Rin * Rin - far * far, 0.0f)) - g.margin;
+                if (hin > 0.0f) {
+                    const int ix0 = max(static_cast<int>(ceilf((tx - hin) * g.inv_sx)), max(bx0, 1));
+                    const int ix1 = min(static_cast<int>(floorf((tx + hin) * g.inv_sx)) - 1, min(bx1, fw - 2));
+                    if (ix0 <= ix1) inner = cell_start[row + ix1 + 1] - cell_start[row + ix0];
+                }
+            }
+            tests += (s3 - s0) - inner;
+        }
+    }
+    // One atomic per warp and counter.
+    for (int o = 16; o > 0; o >>= 1) {
+        rows += __shfl_xor_sync(0xFFFFFFFFu, rows, o);
+        tests += __shfl_xor_sync(0xFFFFFFFFu, tests, o);
+        probed += __shfl_xor_sync(0xFFFFFFFFu, probed, o);
+    }
+    if ((threadIdx.x & 31) == 0 && probed) {
+        atomicAdd(&out[0], static_cast<unsigned long long>(rows));
+        atomicAdd(&out[1], static_cast<unsigned long long>(tests));
+        atomicAdd(&out[2], static_cast<unsigned long long>(probed));
+    }
+}
+
+void launch_search_probe(const float2* rec, const uint32_t* tag, const uint32_t* cell_start, uint32_t n,
+                         const Grid& g, uint32_t stride, unsigned long long* out, cudaStream_t s) {
+    cudaMemsetAsync(out, 0, 3 * sizeof(unsigned long long), s);
+    if (n == 0 || stride == 0) return;
+    const uint32_t probes = (n + stride - 1) / stride;
+    search_probe_kernel<<<div_up(probes, 256), 256, 0, s>>>(rec, tag, cell_start, n, g, stride, out);
+}
+
 void launch_scatter(const ScatterArgs& a, cudaStream_t s) {
     if (a.n == 0) return;
     scatter_kernel<<<div_up(a.n, 256), 256, 0, s>>>(a);

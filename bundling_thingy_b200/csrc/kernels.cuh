@@ -114,6 +114,13 @@ struct MeanArgs {
 };
 void launch_neighbor_mean(const MeanArgs& a, cudaStream_t s);
 
+// Sampled work of the neighbour search under grid g (slot order rec/tag with
+// its cell table): over every `stride`-th slot that is movable, out[0] =
+// search rows, out[1] = samples in boundary cells (tested exactly), out[2] =
+// slots probed (out is cleared first, on s).
+void launch_search_probe(const float2* rec, const uint32_t* tag, const uint32_t* cell_start, uint32_t n,
+                         const Grid& g, uint32_t stride, unsigned long long* out, cudaStream_t s);
+
 // Tiles of the cell table (search cells) and of the slot prefix (slots).
 constexpr uint32_t kCellTile = static_cast<uint32_t>(scan_tile<uint32_t>());
 constexpr uint32_t kPrefixTile = static_cast<uint32_t>(scan_tile<LL2>());
