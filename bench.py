@@ -210,13 +210,13 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum: 99.60 + 49.79 MB)
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum: 82.25 + 44.56 MB)
 # of one launch of the neighbour-mean kernel on the large workload, iteration
 # 15 of a job, from one ncu capture (1 pass) of this kernel on B200:
 #   ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum \
 #       --clock-control none -k regex:neighbor_mean -s 14 -c 1 \
 #       python bench.py --quick --steps 1 --warmup 0 --steady-iterations 0
-MEAN_TRAFFIC_BYTES = 149_390_000
+MEAN_TRAFFIC_BYTES = 126_810_000
 
 
 def workload(edges: int):
@@ -415,7 +415,8 @@ def run_ours(args, ranks: Ranks):
             "step": f"one job: iterations 1-{iters} after an upload (the upload before each step is not timed)",
             "samples": n, "edges": w.edges, "grid": [w.width, w.height], "radius": w.radius, "sigma": w.sigma,
             "search_cells_per_grid_cell": {"x": info.fine_cells_x, "y": info.fine_cells,
-                                           "chosen": "at upload from the graph's density"},
+                                           "chosen": "at upload from the graph's density; re-chosen by the "
+                                                     "search-shape checks after iterations 5, 10 and 20"},
             "iterations_per_job": iters,
             "parallelism": f"replicas x{ranks.world}", "l2": "inputs larger than L2 (~330 MB working set per step)",
         },

@@ -869,13 +869,13 @@ bt_status reshape(bt_ctx* c, uint32_t ky, uint32_t kx) {
 // workload 2-texel rows are fastest at first and 4-texel rows from about the
 // tenth iteration). After 5, 10, 20, 40, ... iterations of an upload, the
 // synchronous calls (bt_iterate, bt_iterate_timed) count the search rows and
-// the boundary samples of every 16th slot under the current shape, predict
+// the boundary samples of every 64th slot under the current shape, predict
 // the best row height and re-bin when the prediction saves more than 8%.
 // The cost model: per sample, kRowCost exact tests' worth per search row
 // (about 2R / sy + 1 rows) plus the boundary samples, whose count scales with
 // the band's width sy + sx. kRowCost is fitted to per-iteration times of five
 // shapes on the large workload at iterations 1 and 30.
-constexpr uint32_t kProbeStride = 16;
+constexpr uint32_t kProbeStride = 64;
 constexpr double kRowCost = 10.0;
 constexpr double kReshapeGain = 0.92;
 
