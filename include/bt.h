@@ -138,16 +138,23 @@ bt_status bt_upload_graph(bt_ctx* ctx, const bt_graph* graph, uint32_t* out_samp
 /* Gpu::iterate (src/gpu.rs:527-553), n times: neighbour mean fused with the
  * density splat, grid rebuild, blur and normalisation (or, with advect_step,
  * one density-gradient advection step fused with the splat, then blur and
- * normalisation). Returns after the work has finished on the device. */
+ * normalisation). Returns after the work has finished on the device.
+ * Unless the options fix the search cells (fine_cells, fine_cells_x), it
+ * checks the search-cell shape after 5, 10, 20, 40, ... iterations of an
+ * upload: a sampled count of the search's rows and boundary samples, one host
+ * wait, and a re-binning when a cost model predicts a saving of more than
+ * 8%. Results do not depend on the shape. */
 bt_status bt_iterate(bt_ctx* ctx, uint32_t n);
 
-/* Enqueue n iterations without waiting (bt_synchronize waits). */
+/* Enqueue n iterations without waiting (bt_synchronize waits). Makes no
+ * search-shape checks (they wait on the host). */
 bt_status bt_iterate_async(bt_ctx* ctx, uint32_t n);
 bt_status bt_synchronize(bt_ctx* ctx);
 
 /* bt_iterate, also returning the device milliseconds between CUDA events
  * recorded on the context's stream before and after the n iterations (the
- * reference logs per-pass gpu_ms, src/profiling.rs:127-133). */
+ * reference logs per-pass gpu_ms, src/profiling.rs:127-133); the search-shape
+ * checks that fall due are inside that span. */
 bt_status bt_iterate_timed(bt_ctx* ctx, uint32_t n, float* device_ms);
 
 bt_status bt_get_info(bt_ctx* ctx, bt_info* info);
