@@ -210,13 +210,13 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum: 82.25 + 44.56 MB)
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum: 99.60 + 49.79 MB)
 # of one launch of the neighbour-mean kernel on the large workload, iteration
 # 15 of a job, from one ncu capture (1 pass) of this kernel on B200:
 #   ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum \
 #       --clock-control none -k regex:neighbor_mean -s 14 -c 1 \
 #       python bench.py --quick --steps 1 --warmup 0 --steady-iterations 0
-MEAN_TRAFFIC_BYTES = 126_810_000
+MEAN_TRAFFIC_BYTES = 149_390_000
 
 
 def workload(edges: int):
@@ -354,6 +354,22 @@ def run_ours(args, ranks: Ranks):
         steady_ms = ranks.max(gpu.iterate_timed(args.steady_iterations))
     gpu.close()
 
+    # The same jobs with the search-shape checks option (off by default).
+    checks_ms = checks_value = None
+    if args.steps:
+        chk = bt.Gpu(bt.Options(width=w.width, height=w.height, neighbor_radius=w.radius, sample_spacing=w.spacing,
+                                blur_sigma=w.sigma, device=device, shape_checks=True))
+        chk.upload((w.xy, w.starts))
+        chk.iterate(iters)
+        ranks.barrier()
+        jobs = []
+        for _ in range(min(args.steps, 5)):
+            chk.upload((w.xy, w.starts))
+            jobs.append(chk.iterate_timed(iters))
+        chk.close()
+        checks_ms = ranks.max(sum(jobs) / len(jobs))
+        checks_value = ranks.sum(float(n) * iters) / (checks_ms / 1e3)
+
     # Stage split of one job (per-stage CUDA events; the iterations run as
     # direct launches instead of a CUDA graph): iteration 1 alone, then 2-30.
     st = bt.Gpu(bt.Options(width=w.width, height=w.height, neighbor_radius=w.radius, sample_spacing=w.spacing,
@@ -415,12 +431,15 @@ def run_ours(args, ranks: Ranks):
             "step": f"one job: iterations 1-{iters} after an upload (the upload before each step is not timed)",
             "samples": n, "edges": w.edges, "grid": [w.width, w.height], "radius": w.radius, "sigma": w.sigma,
             "search_cells_per_grid_cell": {"x": info.fine_cells_x, "y": info.fine_cells,
-                                           "chosen": "at upload from the graph's density; re-chosen by the "
-                                                     "search-shape checks after iterations 5, 10 and 20"},
+                                           "chosen": "at upload from the graph's density"},
             "iterations_per_job": iters,
             "parallelism": f"replicas x{ranks.world}", "l2": "inputs larger than L2 (~330 MB working set per step)",
         },
         "ms_per_iteration": ms_max / args.steps / iters,
+        "shape_checks_option": None if checks_ms is None else {
+            "value": checks_value, "unit": UNIT, "ms_per_job": checks_ms,
+            "note": "same jobs with options.shape_checks = 1 (off by default: 4% faster here, slower on "
+                    "small-radius graphs)"},
         "steady_state": None if steady_ms is None else {
             "value": ranks.sum(float(n) * args.steady_iterations) / (steady_ms / 1e3), "unit": UNIT,
             "ms_per_iteration": steady_ms / args.steady_iterations,

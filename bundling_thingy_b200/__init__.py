@@ -67,7 +67,7 @@ class _Options(ctypes.Structure):
         ("record_neighbors", ctypes.c_uint32), ("search_mode", ctypes.c_uint32), ("fine_cells_x", ctypes.c_uint32),
         ("palette", ctypes.c_uint32), ("msaa", ctypes.c_uint32), ("endpoint_dots", ctypes.c_uint32),
         ("advect_step", ctypes.c_float), ("advect_smooth", ctypes.c_float), ("wait_seconds", ctypes.c_float),
-        ("reserved_options", ctypes.c_uint32),
+        ("shape_checks", ctypes.c_uint32),
     ]
 
 
@@ -134,6 +134,8 @@ SIGNATURES = {
     "bt_read_density_raw": ([_vp, _f32p, ctypes.c_size_t, _f32p], ctypes.c_int32),
     "bt_read_counts": ([_vp, _u32p, ctypes.c_size_t], ctypes.c_int32),
     "bt_read_cells": ([_vp, _u32p, ctypes.c_size_t], ctypes.c_int32),
+    "bt_search_stats": ([_vp, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64),
+                         ctypes.POINTER(ctypes.c_uint64)], ctypes.c_int32),
     "bt_read_binning": ([_vp, _u32p, ctypes.c_size_t, _u32p, ctypes.c_size_t], ctypes.c_int32),
     "bt_read_neighbors": ([_vp, _u32p, ctypes.c_size_t], ctypes.c_int32),
     "bt_distortion": ([_vp, ctypes.c_uint32, _f64p, _f64p], ctypes.c_int32),
@@ -255,6 +257,7 @@ class Options:
     advect_step: float = 0.0     # > 0: density-gradient advection (texels per iteration) instead of the mean
     advect_smooth: float = 0.0   # its Laplacian relaxation along the path, in [0, 1]
     wait_seconds: float = 0.0    # host deadline of blocking calls (0 = 60 s, Gpu::wait, src/gpu.rs:484-490)
+    shape_checks: bool = False   # re-check the search-cell shape during a job (iterate / iterate_timed)
 
     def _struct(self) -> _Options:
         o = _Options()
@@ -280,6 +283,7 @@ class Options:
         o.advect_step = float(self.advect_step)
         o.advect_smooth = float(self.advect_smooth)
         o.wait_seconds = float(self.wait_seconds)
+        o.shape_checks = int(bool(self.shape_checks))
         return o
 
     def resample_scale(self) -> tuple[float, float]:
@@ -503,6 +507,13 @@ class Gpu:
         starts = np.zeros(cells + 1, np.uint32)
         self._ck(library().bt_read_binning(self._h, _p(slots, _u32p), slots.size, _p(starts, _u32p), starts.size))
         return slots, starts
+
+    def search_stats(self, stride: int = 1) -> tuple[int, int, int]:
+        """(search rows, samples in boundary cells, movable samples counted)
+        of the next iteration's neighbour search over every `stride`-th slot."""
+        r, b, p = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+        self._ck(library().bt_search_stats(self._h, int(stride), ctypes.byref(r), ctypes.byref(b), ctypes.byref(p)))
+        return int(r.value), int(b.value), int(p.value)
 
     def read_neighbors(self) -> np.ndarray:
         out = np.zeros(self.info().samples, np.uint32)

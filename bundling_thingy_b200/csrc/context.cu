@@ -433,6 +433,7 @@ bt_status validate_options(const bt_options* o, bt_ctx* c) {
         return fail(c, BT_ERR_INVALID, "invalid sample spacing");
     if (o->neighbor_radius > 0 && (o->fine_cells > 4096 || o->fine_cells_x > 4096))
         return fail(c, BT_ERR_INVALID, "fine_cells too large");
+    if (o->shape_checks > 1) return fail(c, BT_ERR_INVALID, "shape_checks must be 0 or 1");
     if (o->search_mode > 1) return fail(c, BT_ERR_INVALID, "unknown search_mode");
     if (o->palette > BT_PALETTE_BATLOW) return fail(c, BT_ERR_INVALID, "unknown palette");
     if (!(o->advect_step >= 0.0f) || !std::isfinite(o->advect_step) || !(o->advect_smooth >= 0.0f) ||
@@ -863,18 +864,22 @@ bt_status reshape(bt_ctx* c, uint32_t ky, uint32_t kx) {
     return BT_OK;
 }
 
-// Search-shape checks during a job. Early iterations test many boundary
-// samples per search row and favour low rows; as a graph bundles its
-// boundary bands empty, the rows dominate and tall rows win (on the large
-// workload 2-texel rows are fastest at first and 4-texel rows from about the
-// tenth iteration). After 5, 10, 20, 40, ... iterations of an upload, the
-// synchronous calls (bt_iterate, bt_iterate_timed) count the search rows and
-// the boundary samples of every 64th slot under the current shape, predict
-// the best row height and re-bin when the prediction saves more than 8%.
-// The cost model: per sample, kRowCost exact tests' worth per search row
-// (about 2R / sy + 1 rows) plus the boundary samples, whose count scales with
-// the band's width sy + sx. kRowCost is fitted to per-iteration times of five
-// shapes on the large workload at iterations 1 and 30.
+// Search-shape checks during a job (options.shape_checks). Early iterations
+// test many boundary samples per search row and favour low rows; as a graph
+// bundles its boundary bands empty, the rows dominate and tall rows win (on
+// the large workload 2-texel rows are fastest at first and 4-texel rows from
+// about the tenth iteration). After 5, 10, 20, 40, ... iterations of an
+// upload, the synchronous calls (bt_iterate, bt_iterate_timed) count the
+// search rows and the boundary samples of every 64th slot under the current
+// shape, predict the best row height and re-bin when the prediction saves
+// more than 8%. The cost model: per sample, kRowCost exact tests' worth per
+// search row (about 2R / sy + 1 rows) plus the boundary samples, whose count
+// scales with the band's width sy + sx. kRowCost is fitted to per-iteration
+// times of five shapes on the large workload at iterations 1 and 30. Fitted
+// over eight graphs the ratio ranges from 4.8 to 8.4, and no single value
+// chooses well on all of them (30-iteration jobs 4% faster on the large
+// workload, up to 15% slower on small-radius graphs), so the checks are an
+// option, off by default.
 constexpr uint32_t kProbeStride = 64;
 constexpr double kRowCost = 10.0;
 constexpr double kReshapeGain = 0.92;
@@ -1060,7 +1065,7 @@ bt_status bt_iterate_async(bt_ctx* c, uint32_t n) { return iterate_enqueue(c, n,
 // on the way (check_shape).
 bt_status iterate_checked(bt_ctx* c, uint32_t n) {
     if (!c || !c->uploaded) return iterate_enqueue(c, n, true);   // its errors
-    const bool checks = c->has_grid && c->opt.advect_step <= 0.0f && adaptive(c);
+    const bool checks = c->opt.shape_checks && c->has_grid && c->opt.advect_step <= 0.0f && adaptive(c);
     c->stage_used = 0;
     if (n == 0) return iterate_enqueue(c, 0, false);
     while (n > 0) {
@@ -1305,6 +1310,22 @@ bt_status bt_read_cells(bt_ctx* c, uint32_t* dst, size_t count) {
     bt::launch_grid_cells(c->sorted_rec[c->cur].as<float2>(), c->sorted_tag[c->cur].as<uint32_t>(), c->samples,
                           c->grid, c->records.as<uint32_t>(), c->stream);
     return copy_out(c, dst, c->records.p, 4 * count);
+}
+
+bt_status bt_search_stats(bt_ctx* c, uint32_t stride, uint64_t* rows, uint64_t* boundary, uint64_t* probed) {
+    if (bt_status s = need_graph(c)) return s;
+    if (!c->has_grid) return fail(c, BT_ERR_NOT_CONFIGURED, "neighbor radius is not configured");
+    if (!rows || !boundary || !probed || stride == 0) return fail(c, BT_ERR_INVALID, "null argument or zero stride");
+    if (c->opt.advect_step > 0.0f) return fail(c, BT_ERR_NOT_CONFIGURED, "the advection mode has no neighbour search");
+    bt::launch_search_probe(c->sorted_rec[c->cur].as<float2>(), c->sorted_tag[c->cur].as<uint32_t>(),
+                            c->cell_start.as<uint32_t>(), c->samples, c->grid, stride,
+                            c->probe.as<unsigned long long>(), c->stream);
+    BT_CUDA(c, cudaMemcpyAsync(c->h_totals + 5, c->probe.p, 24, cudaMemcpyDeviceToHost, c->stream));
+    if (bt_status s = wait(c)) return s;
+    *rows = c->h_totals[5];
+    *boundary = c->h_totals[6];
+    *probed = c->h_totals[7];
+    return BT_OK;
 }
 
 bt_status bt_read_binning(bt_ctx* c, uint32_t* slot_samples, size_t count, uint32_t* cell_starts, size_t cell_count) {

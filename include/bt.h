@@ -85,7 +85,9 @@ typedef struct bt_options {
        device (a later bt_synchronize can still wait for it). 0 = 60 s, the
        reference's Gpu::wait (src/gpu.rs:484-490). */
     float wait_seconds;
-    uint32_t reserved_options;      /* keep 0 */
+    /* 1: bt_iterate and bt_iterate_timed re-check the search-cell shape during
+       a job (see bt_iterate); 0 (default): the shape chosen at upload stays. */
+    uint32_t shape_checks;
 } bt_options;
 
 typedef struct bt_info {
@@ -139,11 +141,11 @@ bt_status bt_upload_graph(bt_ctx* ctx, const bt_graph* graph, uint32_t* out_samp
  * density splat, grid rebuild, blur and normalisation (or, with advect_step,
  * one density-gradient advection step fused with the splat, then blur and
  * normalisation). Returns after the work has finished on the device.
- * Unless the options fix the search cells (fine_cells, fine_cells_x), it
- * checks the search-cell shape after 5, 10, 20, 40, ... iterations of an
- * upload: a sampled count of the search's rows and boundary samples, one host
- * wait, and a re-binning when a cost model predicts a saving of more than
- * 8%. Results do not depend on the shape. */
+ * With options.shape_checks (and search cells not fixed by fine_cells,
+ * fine_cells_x), it checks the search-cell shape after 5, 10, 20, 40, ...
+ * iterations of an upload: a sampled count of the search's rows and boundary
+ * samples, one host wait, and a re-binning when a cost model predicts a
+ * saving of more than 8%. Results do not depend on the shape. */
 bt_status bt_iterate(bt_ctx* ctx, uint32_t n);
 
 /* Enqueue n iterations without waiting (bt_synchronize waits). Makes no
@@ -194,6 +196,12 @@ bt_status bt_read_counts(bt_ctx* ctx, uint32_t* dst, size_t count);
 /* Neighbour-grid cell ids (spatial_grid.wgsl:67-70) of the current samples,
  * sample order. Requires a configured radius. */
 bt_status bt_read_cells(bt_ctx* ctx, uint32_t* dst, size_t count);
+/* No counterpart in the reference. Work of the next iteration's neighbour
+ * search under the current search cells, over every `stride`-th slot (1 =
+ * all): search rows, samples in boundary cells (tested one by one; the
+ * interior cells come from prefix sums) and movable samples counted. The
+ * search-shape checks of bt_iterate use the same count. */
+bt_status bt_search_stats(bt_ctx* ctx, uint32_t stride, uint64_t* rows, uint64_t* boundary, uint64_t* probed);
 /* The grid binning that the next iteration will search: samples listed by
  * search cell (slot order, `count` = samples) and the start slot of each
  * search cell (cell_count = fine grid cells + 1). */
