@@ -188,6 +188,8 @@ void launch_neighbor_mean(const MeanArgs& a, cudaStream_t s) {
     neighbor_mean_kernel<<<grid, 128, 0, s>>>(a);
 }
 
+namespace {
+
 // Work of the neighbour search on every `stride`-th slot: its search rows
 // and the samples of its boundary cells (those the mean tests exactly), with
 // the row bounds of mean_sample. out[0] += rows, out[1] += boundary samples,
@@ -246,11 +248,13 @@ __global__ void __launch_bounds__(256) search_probe_kernel(const float2* rec, co
     }
 }
 
+}  // namespace
+
 void launch_search_probe(const float2* rec, const uint32_t* tag, const uint32_t* cell_start, uint32_t n,
                          const Grid& g, uint32_t stride, unsigned long long* out, cudaStream_t s) {
     cudaMemsetAsync(out, 0, 3 * sizeof(unsigned long long), s);
     if (n == 0 || stride == 0) return;
-    const uint32_t probes = (n + stride - 1) / stride;
+    const uint64_t probes = (static_cast<uint64_t>(n) + stride - 1) / stride;   // >= 1, <= n
     search_probe_kernel<<<div_up(probes, 256), 256, 0, s>>>(rec, tag, cell_start, n, g, stride, out);
 }
 
