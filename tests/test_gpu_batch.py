@@ -99,6 +99,26 @@ def test_first_slot_matches_oracle(oracle):
     np.testing.assert_array_equal(batch.slot(slot).read_density(), ora.normalized())
 
 
+def test_every_mixed_slot_matches_oracle(oracle):
+    # Each slot of the mixed batch in the persistent step against the oracle's
+    # own run of its graph: maps of 512^2 to 2048^2, radii 1 to 8, both search
+    # modes, density on and off, shrinking and constant sigma.
+    jobs = mixed_jobs()
+    batch = bt.Batch(solo_samples=PERSISTENT)
+    slots = [batch.add(o, w.xy, w.starts) for w, o in jobs]
+    batch.iterate(3)
+    for (w, o), (slot, n) in zip(jobs, slots):
+        ora = oracle.Pipeline(oracle_config(oracle, o))
+        assert ora.upload(w.xy, w.starts) == n
+        ora.iterate(3)
+        xy, ids = batch.slot(slot).read_points()
+        oxy, oids = ora.points()
+        np.testing.assert_array_equal(ids, oids)
+        np.testing.assert_array_equal(xy, oxy)
+        if o.color_by == bt.COLOR_BY_DENSITY:
+            np.testing.assert_array_equal(batch.slot(slot).read_density(), ora.normalized())
+
+
 @pytest.mark.parametrize("solo_samples", POLICIES + [200000])
 def test_slots_join_and_leave_between_iterations(solo_samples):
     # 200000: the small graphs in the persistent step, the mid one on its own.
