@@ -8,6 +8,8 @@ import pytest
 import bundling_thingy_b200 as bt
 from bundling_thingy_b200 import synthetic
 
+from conftest import oracle_config
+
 pytestmark = pytest.mark.gpu
 
 
@@ -85,6 +87,32 @@ def test_requests_in_the_mix_match_standalone_runs(solo_samples):
     for w, o, iters in mixed_requests()[:3]:
         expected2[server.submit(o, w.xy, w.starts, iters)] = (w, o, iters)
     drain(server, len(expected2), expected2)
+    server.close()
+
+
+@pytest.mark.parametrize("solo_samples", [1, 2**32 - 1])
+def test_served_results_match_oracle(oracle, solo_samples):
+    # Every request of the mix against the oracle's own run of its graph, with
+    # all requests on their own contexts (1) or all in the batch (2^32 - 1).
+    server = bt.Server(max_active=8, solo_samples=solo_samples)
+    expected = {}
+    for w, o, iters in mixed_requests()[:5]:
+        expected[server.submit(o, w.xy, w.starts, iters)] = (w, o, iters)
+    for _ in range(len(expected)):
+        r = server.next(60.0)
+        assert r.status == 0, r.message
+        w, o, iters = expected[r.id]
+        ora = oracle.Pipeline(oracle_config(oracle, o))
+        assert ora.upload(w.xy, w.starts) == r.samples
+        if iters:
+            ora.iterate(iters)
+        xy, ids = server.read_points(r.id, r.samples)
+        oxy, oids = ora.points()
+        np.testing.assert_array_equal(ids, oids)
+        np.testing.assert_array_equal(xy, oxy)
+        if o.color_by == bt.COLOR_BY_DENSITY:
+            np.testing.assert_array_equal(server.result(r.id).read_density(), ora.normalized())
+        server.release(r.id)
     server.close()
 
 
